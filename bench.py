@@ -1,0 +1,353 @@
+"""Benchmark of the FDTD (Yee) hot path on B200.
+
+Workload (one bench "step"): the plain-FDTD-with-monitors configuration -- a 256 x 256 x 256
+FP32 vacuum grid (Ca = Da = 1, Cb = Db = dt/dx = 0.5), a Gaussian-modulated Jz point source
+at the centre (centre period 20 steps, width 10, delay 40), an FP64 running-DFT monitor of Ez
+on the plane z = 128 at 8 frequencies over the source band, 1000 time steps from zero fields.
+Synthetic inputs with those shapes; fields (1.2 GB) exceed the 126 MB L2, so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Metric: Gcell-updates/s (Nx*Ny*Nz*T / s, boundary cells included, as the reference counts,
+gDiamond/gdiamond.hpp:1253).  `value` times the device-resident run (CUDA events on the
+launching stream, max over ranks); `e2e` times the same run through the C-ABI with host
+buffers: coefficient upload (12 FP32 arrays from pinned memory), reset, 1000 steps, download
+of the 6 fields and the monitor sums.  Under torchrun each rank runs its own replica (the grid
+is one object; no data-path collective): `scaling` is weak.
+
+--impl reference times the reference's own CPU path, gDiamond::update_FDTD_omp, compiled from
+the reference sources (oracle/_ref/libgdref.so) on this host's cores, on a bounded number of
+time steps of the same 256^3 grid; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (256, 256, 256)
+T_STEPS = 1000
+N_FREQS = 8
+MON_K = 128
+B_ALG = 96  # algorithmic bytes per FP32 cell-update (6 fields r+w, 12 coefficients r)
+WORKLOAD = "fdtd3d_256cube_vacuum_gaussJz_T1000_dft8_zplane"
+METRIC = "Gcell-updates/s"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), \
+        int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        load = [v for v in sm if mx and v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def traffic_from_profile(cfg):
+    """DRAM bytes per launch of the tiled kernel from the committed ncu summary, if the
+    summary's configuration matches the one running now."""
+    p = os.path.join(ROOT, "profiles", "fdtd_tiled_256cube_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    kv = {}
+    for ln in open(p):
+        if "=" in ln and not ln.startswith("#"):
+            k, v = ln.split("=", 1)
+            kv[k.strip()] = v.strip()
+    try:
+        if (int(kv["blt"]), int(kv["tile_rows"]), int(kv["z_chunks"])) != \
+                (cfg["blt"], cfg["tile_rows"], cfg["z_chunks"]):
+            return None
+        return float(kv["dram_bytes_per_launch"])
+    except (KeyError, ValueError):
+        return None
+
+
+# ------------------------------------------------------------------ reference arm / CPU
+
+
+def cpu_reference_sample(target_s=8.0, max_T=64):
+    """Times the reference's update_FDTD_omp on the 256^3 grid for a bounded number of steps.
+    Returns (Gcell/s, cores, sample description, seconds, T)."""
+    import oracle
+    r = oracle.Reference(*SHAPE)
+    t1 = r.run_omp(1)
+    T = int(max(1, min(max_T, target_s / max(t1, 1e-3))))
+    secs = r.run_omp(T)
+    cores = oracle.ref().gdref_max_threads()
+    r.close()
+    n = SHAPE[0] * SHAPE[1] * SHAPE[2]
+    return n * T / secs / 1e9, cores, T, secs
+
+
+def run_reference_arm(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libgdref.so not built"}))
+        return 0
+    r = oracle.Reference(*SHAPE)
+    cores = oracle.ref().gdref_max_threads()
+    t1 = r.run_omp(1)
+    T = int(max(1, min(64, 3.0 / max(t1, 1e-3))))  # each step a ~3 s bounded sample
+    for _ in range(args.warmup):
+        r.run_omp(T)
+    secs = [r.run_omp(T) for _ in range(args.steps)]
+    r.close()
+    n = SHAPE[0] * SHAPE[1] * SHAPE[2]
+    total = sum(secs)
+    value = n * T * args.steps / total / 1e9
+    sample = (f"gDiamond::update_FDTD_omp({T}) on the 256^3 grid (reference constructor "
+              f"coefficients and Mz source; same per-cell work as the workload), wall time of "
+              f"the call incl. its temporaries and copy-out; {cores} OpenMP threads")
+    line = {"metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample_timesteps": T, "grid": list(SHAPE)},
+            "cpu_baseline": {"value": value, "unit": "Gcell-updates/s", "cores": cores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+
+
+def run_ours(args):
+    import torch
+    import gdiamond_b200 as gd
+    from gdiamond_b200 import workloads as W
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    nx, ny, nz = SHAPE
+    ncell = nx * ny * nz
+    coefs = W.vacuum_coefficients(SHAPE)
+    wave = W.gaussian_wave(T_STEPS)
+    freqs = W.source_band(N_FREQS)
+    src = [dict(component="Jz", wave=wave, i=nx // 2, j=ny // 2, k=nz // 2)]
+
+    sim = gd.Simulation(nx, ny, nz, device=local)
+    sim.set_coefficients(coefs)
+    sim.set_sources(src)
+    mid = sim.add_dft_monitor("Ez", MON_K, freqs, scale=1.0)
+    stream = torch.cuda.Stream()
+
+    def one_step():
+        sim.reset()
+        sim.step(T_STEPS, stream=stream)
+
+    # warm-up (the first step also runs the autotuner)
+    for _ in range(max(args.warmup, 1)):
+        one_step()
+    stream.synchronize()
+    sim.sync()
+    cfg = sim.config()
+    launches_per_step = cfg["launches"]
+
+    # ---------------- device-resident timed region
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        sim.reset()
+        ev[k][0].record(stream)
+        sim.step(T_STEPS, stream=stream)
+        ev[k][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    sim.sync()
+    total_ms = max_over_ranks(t_start.elapsed_time(t_end))
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    ms_per_step = total_ms / args.steps
+    value = world * ncell * T_STEPS * args.steps / (total_ms / 1e3) / 1e9
+    launch_ms = statistics.mean(kern_ms) / launches_per_step
+
+    # ---------------- end to end through the C-ABI with host buffers
+    pinned = [torch.empty(ncell, dtype=torch.float32, pin_memory=True).numpy() for _ in range(12)]
+    for a in range(12):
+        pinned[a][:] = coefs[a]
+    fields_out = [torch.empty(ncell, dtype=torch.float32, pin_memory=True).numpy()
+                  for _ in range(6)]
+
+    def e2e_step():
+        sim.set_coefficients(pinned)
+        sim.reset()
+        sim.step(T_STEPS)
+        for c in range(6):
+            sim.get_field(c, out=fields_out[c])
+        return sim.get_dft(mid)
+
+    e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        re, im = e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * ncell * T_STEPS * args.steps / e2e_s / 1e9
+    h2d = 12 * ncell * 4 + wave.nbytes
+    d2h = 6 * ncell * 4 + re.nbytes + im.nbytes
+
+    # ---------------- roofline of the dominant kernel (the tiled kernel)
+    hbm, kind = peaks()
+    cells_per_launch = ncell * cfg["blt"]
+    achieved = B_ALG * cells_per_launch / (launch_ms / 1e3) / 1e9
+    traffic = traffic_from_profile(cfg)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            gcs, cores, Ts, secs = cpu_reference_sample()
+            cpu = {"value": gcs, "unit": "Gcell-updates/s", "cores": cores, "kind": "reference",
+                   "sample": f"gDiamond::update_FDTD_omp({Ts}) on the 256^3 grid, {secs:.1f} s "
+                             f"wall, {cores} OpenMP threads (reference compiled from its sources)"}
+        except Exception as e:  # the reference build may be absent on a user machine
+            cpu = {"value": None, "unit": "Gcell-updates/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    sim.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded shapes of the workload; no dataset)",
+        "config": {"workload": WORKLOAD, "grid": list(SHAPE), "timesteps": T_STEPS,
+                   "dft_freqs": N_FREQS, "kernel": cfg["kernel"], "blt": cfg["blt"],
+                   "tile_rows": cfg["tile_rows"], "z_chunks": cfg["z_chunks"],
+                   "parallelism": f"replicas{world}",
+                   "l2": "inputs (1.2 GB of fields) larger than L2; no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic,
+                     "note": f"achieved = {B_ALG} B/cell-update x {cells_per_launch} cell-updates "
+                             f"per launch / mean launch time {launch_ms:.4f} ms; peak {kind}; "
+                             f"temporal tiling lets frac exceed 1"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "Gcell-updates/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,261 @@
+"""gdiamond_b200 -- B200-native 3D FDTD (Yee) solver.
+
+Python binding of the C-ABI in ``include/fdtd_capi.h`` (``libgdiamond_b200.so``, built
+in-tree by ``python -m gdiamond_b200.build``).  Every step runs a CUDA kernel through the
+C-ABI; there is no CPU path here, and importing the binding fails loudly when the library
+is missing.
+
+Reference surface mirrored: gdiamond::gDiamond (gDiamond/gdiamond.hpp:17-907) -- a grid of
+Nx x Ny x Nz cells with 12 per-cell coefficient arrays, J/M current sources and
+``update_FDTD_gpu*(num_timesteps)``; results read back per field component.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgdiamond_b200.so")
+
+COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+SOURCE_COMPONENTS = ("Jx", "Jy", "Jz", "Mx", "My", "Mz")
+COEFFS = ("Cax", "Cay", "Caz", "Cbx", "Cby", "Cbz", "Dax", "Day", "Daz", "Dbx", "Dby", "Dbz")
+KERNELS = {"auto": 0, "naive": 1, "tiled": 2}
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
+SRC_POINT, SRC_PLANE_Z = 0, 1
+
+# Every symbol declared in include/fdtd_capi.h.
+EXPORTS = (
+    "fdtd_version", "fdtd_status_string", "fdtd_last_error", "fdtd_create", "fdtd_destroy",
+    "fdtd_set_coefficients", "fdtd_set_coefficients_device", "fdtd_material_count",
+    "fdtd_set_sources", "fdtd_add_dft_monitor", "fdtd_reset", "fdtd_step", "fdtd_sync",
+    "fdtd_get_step", "fdtd_get_field", "fdtd_set_field", "fdtd_get_dft",
+    "fdtd_get_field_device", "fdtd_set_storage_scale", "fdtd_get_config",
+)
+
+
+class FdtdError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+class _Desc(C.Structure):
+    _fields_ = [("nx", C.c_int64), ("ny", C.c_int64), ("nz", C.c_int64), ("dx", C.c_float),
+                ("device", C.c_int32), ("storage", C.c_int32), ("kernel", C.c_int32),
+                ("blt", C.c_int32), ("tile_rows", C.c_int32), ("z_chunks", C.c_int32)]
+
+
+class _Source(C.Structure):
+    _fields_ = [("component", C.c_int32), ("kind", C.c_int32),
+                ("i", C.c_int64), ("j", C.c_int64), ("k", C.c_int64)]
+
+
+_lib = None
+
+
+def library():
+    """The loaded C-ABI library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m gdiamond_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        P, V = C.POINTER, C.c_void_p
+        sig = {
+            "fdtd_version": ([], C.c_char_p),
+            "fdtd_status_string": ([C.c_int], C.c_char_p),
+            "fdtd_last_error": ([V], C.c_char_p),
+            "fdtd_create": ([P(_Desc), P(V)], C.c_int),
+            "fdtd_destroy": ([V], C.c_int),
+            "fdtd_set_coefficients": ([V, P(P(C.c_float))], C.c_int),
+            "fdtd_set_coefficients_device": ([V, P(V)], C.c_int),
+            "fdtd_material_count": ([V, P(C.c_int32)], C.c_int),
+            "fdtd_set_sources": ([V, P(_Source), C.c_int32, P(C.c_float), C.c_int64], C.c_int),
+            "fdtd_add_dft_monitor": ([V, C.c_int32, C.c_int64, P(C.c_double), C.c_int32,
+                                      C.c_double, C.c_double, P(C.c_int32)], C.c_int),
+            "fdtd_reset": ([V], C.c_int),
+            "fdtd_step": ([V, C.c_int64, V], C.c_int),
+            "fdtd_sync": ([V], C.c_int),
+            "fdtd_get_step": ([V, P(C.c_int64)], C.c_int),
+            "fdtd_get_field": ([V, C.c_int32, P(C.c_float)], C.c_int),
+            "fdtd_set_field": ([V, C.c_int32, P(C.c_float)], C.c_int),
+            "fdtd_get_dft": ([V, C.c_int32, P(C.c_double), P(C.c_double)], C.c_int),
+            "fdtd_get_field_device": ([V, C.c_int32, V, V], C.c_int),
+            "fdtd_set_storage_scale": ([V, P(C.c_float)], C.c_int),
+            "fdtd_get_config": ([V, P(C.c_int32)], C.c_int),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _fp(a, T=C.c_float):
+    return a.ctypes.data_as(C.POINTER(T))
+
+
+class Simulation:
+    """One FDTD grid resident on a GPU (a handle of the C-ABI).
+
+    Parameters mirror the reference constructor ``gDiamond(Nx, Ny, Nz)``; ``dx`` is the
+    spacing used in the -J*dx / -M*dx source terms (reference default 0.1,
+    gDiamond/gdiamond.hpp:899).
+    """
+
+    def __init__(self, nx, ny, nz, dx=np.float32(0.1), device=0, kernel="auto", blt=0,
+                 tile_rows=0, z_chunks=0, storage="f32"):
+        self.shape = (int(nx), int(ny), int(nz))
+        self._L = library()
+        d = _Desc(nx, ny, nz, float(np.float32(dx)), device, STORAGE[storage], KERNELS[kernel],
+                  blt, tile_rows, z_chunks)
+        h = C.c_void_p()
+        st = self._L.fdtd_create(C.byref(d), C.byref(h))
+        if st != 0:
+            raise FdtdError(st, self._L.fdtd_last_error(None).decode())
+        self._h = h
+        self._keep = []
+        self.n_monitors = 0
+        self._monitor_nf = []
+
+    # ---------------------------------------------------------------- plumbing
+    def _check(self, st):
+        if st != 0:
+            raise FdtdError(st, self._L.fdtd_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fdtd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def ncells(self):
+        nx, ny, nz = self.shape
+        return nx * ny * nz
+
+    # ---------------------------------------------------------------- set-up
+    def set_coefficients(self, coefs):
+        """12 arrays (Cax..Dbz) of Nx*Ny*Nz float32, host numpy or device torch tensors."""
+        if len(coefs) != 12:
+            raise ValueError("need 12 coefficient arrays")
+        if hasattr(coefs[0], "data_ptr"):  # device tensors
+            arr = (C.c_void_p * 12)(*[int(c.data_ptr()) for c in coefs])
+            self._check(self._L.fdtd_set_coefficients_device(self._h, arr))
+            return
+        cs = [np.ascontiguousarray(c, np.float32).reshape(-1) for c in coefs]
+        for c in cs:
+            if c.size != self.ncells:
+                raise ValueError("coefficient array size mismatch")
+        arr = (C.POINTER(C.c_float) * 12)(*[_fp(c) for c in cs])
+        self._check(self._L.fdtd_set_coefficients(self._h, arr))
+
+    def material_count(self):
+        n = C.c_int32()
+        self._check(self._L.fdtd_material_count(self._h, C.byref(n)))
+        return n.value
+
+    def set_sources(self, sources):
+        """sources: iterable of dicts {component: "Jz", wave: float32[T], i, j, k, kind}."""
+        sources = list(sources)
+        n = len(sources)
+        arr = (_Source * max(n, 1))()
+        tw = max([len(s["wave"]) for s in sources] + [1])
+        waves = np.zeros((max(n, 1), tw), np.float32)
+        for q, s in enumerate(sources):
+            comp = s["component"]
+            comp = SOURCE_COMPONENTS.index(comp) if isinstance(comp, str) else int(comp)
+            arr[q] = _Source(comp, s.get("kind", SRC_POINT), s.get("i", 0), s.get("j", 0), s["k"])
+            waves[q, :len(s["wave"])] = s["wave"]
+        self._keep = [arr, waves]
+        self._check(self._L.fdtd_set_sources(self._h, arr, n, _fp(waves), tw))
+
+    def add_dft_monitor(self, component, k, freqs, scale=1.0, dt=np.float32(0.05)):
+        comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
+        f = np.ascontiguousarray(freqs, np.float64)
+        mid = C.c_int32()
+        self._check(self._L.fdtd_add_dft_monitor(self._h, comp, k, _fp(f, C.c_double), len(f),
+                                                  float(scale), float(np.float32(dt)),
+                                                  C.byref(mid)))
+        self.n_monitors += 1
+        self._monitor_nf.append(len(f))
+        return mid.value
+
+    # ---------------------------------------------------------------- running
+    def reset(self):
+        self._check(self._L.fdtd_reset(self._h))
+
+    def step(self, T, stream=None):
+        """Run T steps asynchronously on `stream` (a torch.cuda.Stream, an int handle or None)."""
+        s = None
+        if stream is not None:
+            s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        self._check(self._L.fdtd_step(self._h, int(T), s))
+
+    def sync(self):
+        self._check(self._L.fdtd_sync(self._h))
+
+    @property
+    def t(self):
+        v = C.c_int64()
+        self._check(self._L.fdtd_get_step(self._h, C.byref(v)))
+        return v.value
+
+    def config(self):
+        out = (C.c_int32 * 5)()
+        self._check(self._L.fdtd_get_config(self._h, out))
+        kernel = {1: "naive", 2: "tiled"}.get(out[0], "none")
+        return {"kernel": kernel, "blt": out[1], "tile_rows": out[2], "z_chunks": out[3],
+                "launches": out[4]}
+
+    # ---------------------------------------------------------------- results
+    def get_field(self, component, out=None):
+        comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
+        if out is None:
+            out = np.empty(self.ncells, np.float32)
+        self._check(self._L.fdtd_get_field(self._h, comp, _fp(out)))
+        return out
+
+    def fields(self):
+        return [self.get_field(c) for c in range(6)]
+
+    def set_field(self, component, values):
+        comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
+        v = np.ascontiguousarray(values, np.float32).reshape(-1)
+        if v.size != self.ncells:
+            raise ValueError("field size mismatch")
+        self._check(self._L.fdtd_set_field(self._h, comp, _fp(v)))
+
+    def get_field_device(self, component, out_ptr, stream=None):
+        comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
+        s = None
+        if stream is not None:
+            s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        self._check(self._L.fdtd_get_field_device(self._h, comp, C.c_void_p(out_ptr), s))
+
+    def get_dft(self, monitor_id):
+        nx, ny, _ = self.shape
+        nf = self._monitor_nf[monitor_id]
+        re = np.empty((nf, ny, nx), np.float64)
+        im = np.empty((nf, ny, nx), np.float64)
+        self._check(self._L.fdtd_get_dft(self._h, monitor_id, _fp(re, C.c_double),
+                                          _fp(im, C.c_double)))
+        return re, im
+
+
+from . import workloads  # noqa: E402,F401

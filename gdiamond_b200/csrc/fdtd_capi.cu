@@ -1,0 +1,703 @@
+// fdtd_capi.cu -- host side of the C-ABI declared in include/fdtd_capi.h.
+//
+// Owns the device state of one grid (two pitched field sets, coefficients as a material map or
+// per-cell arrays, sources, monitors, the device error word), encodes the TMA tensor maps,
+// runs the autotuner and dispatches the naive or tiled kernels.  Nothing here falls back to the
+// CPU: every step runs a CUDA kernel or returns an error status.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/fdtd_capi.h"
+#include "fdtd_kernels.cuh"
+
+using fdtd::Grid;
+using fdtd::Material;
+
+namespace {
+
+constexpr int kMaxMaterials = 65536;
+constexpr double kPiD = 3.14159265358979323846;
+
+enum CoefMode { kCoefNone = 0, kCoefMaterial = 1, kCoefPerCell = 2 };
+
+struct MonitorHost {
+  int comp = 0;
+  long long k = 0;
+  int nf = 0;
+  double scale = 1.0, dt = 0.0;
+  std::vector<double> freqs;
+  double* re = nullptr;  // [nf][ny][nx]
+  double* im = nullptr;
+  double2* tab = nullptr;  // [tab_cap][nf]
+  long long tab_cap = 0;
+};
+
+std::string g_create_error;
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Process-wide autotuning cache keyed by grid shape.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, fdtd::TiledConfig> g_tune_cache;
+
+}  // namespace
+
+struct fdtd_handle {
+  fdtd_desc desc{};
+  Grid g{};
+  size_t cells = 0;  // pitched elements per field array
+  cudaStream_t stream = nullptr;
+  float* F[2][6] = {};
+  int cur = 0;
+  int coef_mode = kCoefNone;
+  float* coef[12] = {};  // pitched per-cell arrays (staging / per-cell mode)
+  uint16_t* mat = nullptr;
+  Material* table = nullptr;
+  int nmat = 0;
+  void* scratch = nullptr;
+  fdtd::SourceDev src[fdtd::kMaxSources] = {};
+  int nsrc = 0;
+  float* d_wave = nullptr;
+  long long tw = 0;
+  MonitorHost mon[fdtd::kMaxMonitors];
+  int nmon = 0;
+  long long t = 0;
+  int* d_err = nullptr;
+  fdtd::TiledConfig cfg{0, 0, 0};
+  bool cfg_ready = false;
+  CUtensorMap maps[2][6];
+  CUtensorMap mat_map;
+  int maps_rows = 0;
+  int last_kernel = 0, last_launches = 0;
+  std::string err;
+};
+
+namespace {
+
+fdtd_status fail(fdtd_handle* h, fdtd_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (h)
+    h->err = buf;
+  else
+    g_create_error = buf;
+  return s;
+}
+
+#define CUDA_TRY(h, call)                                                                    \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail((h), e_ == cudaErrorMemoryAllocation ? FDTD_ERR_OOM : FDTD_ERR_CUDA,       \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int now = -1;
+    cudaGetDevice(&now);
+    if (prev >= 0 && now != prev) cudaSetDevice(prev);
+  }
+};
+
+cudaStream_t pick_stream(fdtd_handle* h, void* s) {
+  return s ? static_cast<cudaStream_t>(s) : h->stream;
+}
+
+fdtd_status encode_map(fdtd_handle* h, CUtensorMap* m, void* base, CUtensorMapDataType dt,
+                       int esz, int box_x, int box_y) {
+  auto enc = get_encode_fn();
+  if (!enc) return fail(h, FDTD_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  const cuuint64_t dims[3] = {(cuuint64_t)h->g.nx, (cuuint64_t)h->g.ny, (cuuint64_t)h->g.nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)h->g.pitch * esz, (cuuint64_t)h->g.plane * esz};
+  const cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(h, FDTD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return FDTD_OK;
+}
+
+fdtd_status ensure_maps(fdtd_handle* h, int rows) {
+  if (h->maps_rows == rows) return FDTD_OK;
+  for (int s = 0; s < 2; ++s)
+    for (int c = 0; c < 6; ++c) {
+      fdtd_status st = encode_map(h, &h->maps[s][c], h->F[s][c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                  4, 32, rows);
+      if (st != FDTD_OK) return st;
+    }
+  fdtd_status st = encode_map(h, &h->mat_map, h->mat, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2,
+                              fdtd::kMatBoxX, rows);
+  if (st != FDTD_OK) return st;
+  h->maps_rows = rows;
+  return FDTD_OK;
+}
+
+fdtd::Sources make_sources(const fdtd_handle* h) {
+  fdtd::Sources S{};
+  S.n = h->nsrc;
+  for (int n = 0; n < h->nsrc; ++n) S.s[n] = h->src[n];
+  S.wave = h->d_wave;
+  S.tw = h->tw;
+  return S;
+}
+
+fdtd::Monitors make_monitors(const fdtd_handle* h) {
+  fdtd::Monitors M{};
+  M.n = h->nmon;
+  for (int m = 0; m < h->nmon; ++m) {
+    const MonitorHost& mh = h->mon[m];
+    M.m[m].comp = mh.comp;
+    M.m[m].k = (int)mh.k;
+    M.m[m].nf = mh.nf;
+    M.m[m].scale = mh.scale;
+    M.m[m].tab = mh.tab;
+    M.m[m].re = mh.re;
+    M.m[m].im = mh.im;
+  }
+  return M;
+}
+
+// The cos/sin table must cover steps [0, upto).
+fdtd_status ensure_tables(fdtd_handle* h, long long upto) {
+  for (int m = 0; m < h->nmon; ++m) {
+    MonitorHost& mh = h->mon[m];
+    if (mh.tab_cap >= upto) continue;
+    long long cap = std::max<long long>(upto, std::max<long long>(1024, mh.tab_cap * 2));
+    std::vector<double2> host((size_t)cap * mh.nf);
+    for (long long t = 0; t < cap; ++t) {
+      const double tt = (double)t * mh.dt;
+      for (int f = 0; f < mh.nf; ++f) {
+        const double w = 2.0 * kPiD * mh.freqs[f];
+        const double ph = w * tt;
+        host[(size_t)t * mh.nf + f] = make_double2(std::cos(ph), std::sin(ph));
+      }
+    }
+    double2* d = nullptr;
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    CUDA_TRY(h, cudaMalloc(&d, host.size() * sizeof(double2)));
+    CUDA_TRY(h, cudaMemcpy(d, host.data(), host.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    if (mh.tab) cudaFree(mh.tab);
+    mh.tab = d;
+    mh.tab_cap = cap;
+  }
+  return FDTD_OK;
+}
+
+fdtd::TiledArgs make_tiled_args(fdtd_handle* h, const fdtd::TiledConfig& c, long long t0,
+                                bool with_io) {
+  fdtd::TiledArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int k = 0; k < 6; ++k) a.tm_src[k] = h->maps[h->cur][k];
+  a.tm_mat = h->mat_map;
+  a.g = h->g;
+  for (int k = 0; k < 6; ++k) a.dst.f[k] = h->F[h->cur ^ 1][k];
+  a.table = h->table;
+  if (with_io) {
+    a.S = make_sources(h);
+    a.M = make_monitors(h);
+  }
+  a.t0 = t0;
+  a.dx = h->desc.dx;
+  a.zlen = (h->g.nz + c.z_chunks - 1) / c.z_chunks;
+  a.err = h->d_err;
+  return a;
+}
+
+// Candidate tiled configurations for the autotuner.
+std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
+  std::vector<fdtd::TiledConfig> out;
+  const int blts[] = {1, 2, 3, 4, 5, 6};
+  const int rows_l[] = {8, 16, 32};
+  const int zc[] = {1, 2, 4, 8};
+  for (int rows : rows_l)
+    for (int b : blts)
+      for (int z : zc) {
+        fdtd::TiledConfig c{b, rows, z};
+        if (!fdtd::tiled_config_supported(c)) continue;
+        if (h->desc.blt > 0 && b != h->desc.blt) continue;
+        if (h->desc.tile_rows > 0 && rows != h->desc.tile_rows) continue;
+        if (h->desc.z_chunks > 0 && z != h->desc.z_chunks) continue;
+        if ((h->g.nz + z - 1) / z < 2 * b) continue;  // chunk shorter than its halo
+        out.push_back(c);
+      }
+  return out;
+}
+
+// Times every candidate on the current field set (source set -> scratch destination; sources
+// and monitors off, so the simulation state is not changed) and keeps the fastest per step.
+fdtd_status autotune(fdtd_handle* h, cudaStream_t st) {
+  const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz,
+                                   h->desc.blt * 10000 + h->desc.tile_rows * 100 + h->desc.z_chunks);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      h->cfg = it->second;
+      h->cfg_ready = true;
+      return FDTD_OK;
+    }
+  }
+  std::vector<fdtd::TiledConfig> cands = candidates(h);
+  if (cands.empty()) return fail(h, FDTD_ERR_UNSUPPORTED, "no tiled configuration fits this grid");
+  if (cands.size() == 1) {
+    h->cfg = cands[0];
+    h->cfg_ready = true;
+    return FDTD_OK;
+  }
+  cudaEvent_t e0, e1;
+  CUDA_TRY(h, cudaEventCreate(&e0));
+  CUDA_TRY(h, cudaEventCreate(&e1));
+  float best = 1e30f;
+  fdtd::TiledConfig best_c = cands[0];
+  const int reps = 2;
+  for (const auto& c : cands) {
+    fdtd_status s = ensure_maps(h, c.rows);
+    if (s != FDTD_OK) return s;
+    const fdtd::TiledArgs a = make_tiled_args(h, c, 0, false);
+    CUDA_TRY(h, fdtd::launch_tiled(c, a, h->g, st));  // warm-up
+    CUDA_TRY(h, cudaEventRecord(e0, st));
+    for (int r = 0; r < reps; ++r) CUDA_TRY(h, fdtd::launch_tiled(c, a, h->g, st));
+    CUDA_TRY(h, cudaEventRecord(e1, st));
+    CUDA_TRY(h, cudaEventSynchronize(e1));
+    float ms = 0;
+    CUDA_TRY(h, cudaEventElapsedTime(&ms, e0, e1));
+    const float per_step = ms / (reps * c.blt);
+    if (per_step < best) {
+      best = per_step;
+      best_c = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->cfg = best_c;
+  h->cfg_ready = true;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = best_c;
+  return FDTD_OK;
+}
+
+fdtd_status check_device_error(fdtd_handle* h) {
+  int e = 0;
+  CUDA_TRY(h, cudaMemcpy(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e != fdtd::kErrNone) {
+    cudaMemset(h->d_err, 0, sizeof(int));
+    return fail(h, FDTD_ERR_DEVICE_TIMEOUT,
+                "a device-side bounded wait expired (error word %d); results are invalid", e);
+  }
+  return FDTD_OK;
+}
+
+void free_all(fdtd_handle* h) {
+  for (int s = 0; s < 2; ++s)
+    for (int c = 0; c < 6; ++c) cudaFree(h->F[s][c]);
+  for (int a = 0; a < 12; ++a) cudaFree(h->coef[a]);
+  cudaFree(h->mat);
+  cudaFree(h->table);
+  cudaFree(h->scratch);
+  cudaFree(h->d_wave);
+  cudaFree(h->d_err);
+  for (int m = 0; m < h->nmon; ++m) {
+    cudaFree(h->mon[m].re);
+    cudaFree(h->mon[m].im);
+    cudaFree(h->mon[m].tab);
+  }
+  if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+fdtd_status upload_coefficients(fdtd_handle* h, const float* const* src, cudaMemcpyKind kind) {
+  const size_t bytes = h->cells * sizeof(float);
+  for (int a = 0; a < 12; ++a) {
+    if (!src[a]) return fail(h, FDTD_ERR_INVALID_ARG, "coefficient array %d is NULL", a);
+    if (!h->coef[a]) {
+      CUDA_TRY(h, cudaMalloc(&h->coef[a], bytes));
+      CUDA_TRY(h, cudaMemsetAsync(h->coef[a], 0, bytes, h->stream));
+    }
+    CUDA_TRY(h, cudaMemcpy2DAsync(h->coef[a], (size_t)h->g.pitch * 4, src[a], (size_t)h->g.nx * 4,
+                                  (size_t)h->g.nx * 4, (size_t)h->g.ny * h->g.nz, kind, h->stream));
+  }
+  if (!h->mat) {
+    CUDA_TRY(h, cudaMalloc(&h->mat, h->cells * sizeof(uint16_t)));
+    CUDA_TRY(h, cudaMemsetAsync(h->mat, 0, h->cells * sizeof(uint16_t), h->stream));
+    CUDA_TRY(h, cudaMalloc(&h->table, kMaxMaterials * sizeof(Material)));
+    CUDA_TRY(h, cudaMalloc(&h->scratch, fdtd::material_scratch_bytes()));
+  }
+  fdtd::DedupResult r{};
+  CUDA_TRY(h, fdtd::build_material_map(h->g, h->coef, h->mat, h->table, h->scratch,
+                                       fdtd::material_scratch_bytes(), h->stream, &r));
+  if (r.ok) {
+    h->coef_mode = kCoefMaterial;
+    h->nmat = r.nmat;
+  } else {
+    h->coef_mode = kCoefPerCell;
+    h->nmat = 0;
+  }
+  return FDTD_OK;
+}
+
+}  // namespace
+
+// ============================================================================== C-ABI
+
+extern "C" {
+
+const char* fdtd_version(void) { return "gdiamond_b200 0.1 (sm_100a)"; }
+
+const char* fdtd_status_string(fdtd_status s) {
+  switch (s) {
+    case FDTD_OK: return "ok";
+    case FDTD_ERR_INVALID_ARG: return "invalid argument";
+    case FDTD_ERR_OOM: return "out of device memory";
+    case FDTD_ERR_CUDA: return "CUDA error";
+    case FDTD_ERR_UNSUPPORTED: return "unsupported configuration";
+    case FDTD_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+    case FDTD_ERR_NUMERIC: return "numeric check failed";
+  }
+  return "unknown status";
+}
+
+const char* fdtd_last_error(const fdtd_handle* h) {
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
+  if (!d || !out) return fail(nullptr, FDTD_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  if (d->nx < 3 || d->ny < 3 || d->nz < 3)
+    return fail(nullptr, FDTD_ERR_INVALID_ARG, "grid must be at least 3 cells per axis");
+  if (d->nx > (1 << 24) || d->ny > (1 << 24) || d->nz > (1 << 24))
+    return fail(nullptr, FDTD_ERR_INVALID_ARG, "grid axis too large");
+  if (d->storage != FDTD_STORE_F32)
+    return fail(nullptr, FDTD_ERR_UNSUPPORTED, "only FP32 field storage is built");
+  if (d->kernel < FDTD_KERNEL_AUTO || d->kernel > FDTD_KERNEL_TILED)
+    return fail(nullptr, FDTD_ERR_INVALID_ARG, "unknown kernel %d", d->kernel);
+  if (d->blt < 0 || d->blt > 6) return fail(nullptr, FDTD_ERR_INVALID_ARG, "blt must be 0..6");
+  if (d->tile_rows != 0 && d->tile_rows != 8 && d->tile_rows != 16 && d->tile_rows != 32)
+    return fail(nullptr, FDTD_ERR_INVALID_ARG, "tile_rows must be 0, 8, 16 or 32");
+  if (d->z_chunks < 0) return fail(nullptr, FDTD_ERR_INVALID_ARG, "z_chunks must be >= 0");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, FDTD_ERR_CUDA, "no CUDA device available");
+  if (d->device < 0 || d->device >= ndev)
+    return fail(nullptr, FDTD_ERR_INVALID_ARG, "device %d out of range", d->device);
+  DeviceGuard dg(d->device);
+  fdtd_handle* h = new fdtd_handle();
+  h->desc = *d;
+  h->g.nx = (int)d->nx;
+  h->g.ny = (int)d->ny;
+  h->g.nz = (int)d->nz;
+  h->g.pitch = (int)((d->nx + 7) / 8 * 8);
+  h->g.plane = (long long)h->g.pitch * d->ny;
+  h->cells = (size_t)h->g.plane * d->nz;
+  auto bail = [&](fdtd_status s) {
+    g_create_error = h->err;
+    free_all(h);
+    delete h;
+    return s;
+  };
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(h, FDTD_ERR_CUDA, "cudaStreamCreate failed"));
+  for (int s = 0; s < 2; ++s)
+    for (int c = 0; c < 6; ++c) {
+      cudaError_t e = cudaMalloc(&h->F[s][c], h->cells * sizeof(float));
+      if (e != cudaSuccess)
+        return bail(fail(h, FDTD_ERR_OOM, "cudaMalloc of %zu field bytes failed: %s",
+                         h->cells * sizeof(float), cudaGetErrorString(e)));
+      cudaMemsetAsync(h->F[s][c], 0, h->cells * sizeof(float), h->stream);
+    }
+  if (cudaMalloc(&h->d_err, sizeof(int)) != cudaSuccess)
+    return bail(fail(h, FDTD_ERR_OOM, "cudaMalloc failed"));
+  cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return bail(fail(h, FDTD_ERR_CUDA, "initialisation failed"));
+  *out = h;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_destroy(fdtd_handle* h) {
+  if (!h) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_set_coefficients(fdtd_handle* h, const float* const* coef12) {
+  if (!h || !coef12) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  return upload_coefficients(h, coef12, cudaMemcpyHostToDevice);
+}
+
+fdtd_status fdtd_set_coefficients_device(fdtd_handle* h, const float* const* coef12_dev) {
+  if (!h || !coef12_dev) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  return upload_coefficients(h, coef12_dev, cudaMemcpyDeviceToDevice);
+}
+
+fdtd_status fdtd_material_count(const fdtd_handle* h, int32_t* nmat) {
+  if (!h || !nmat) return FDTD_ERR_INVALID_ARG;
+  *nmat = h->coef_mode == kCoefMaterial ? h->nmat : 0;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_set_sources(fdtd_handle* h, const fdtd_source* sources, int32_t nsrc,
+                             const float* waveforms, int64_t T_wave) {
+  if (!h) return FDTD_ERR_INVALID_ARG;
+  if (nsrc < 0 || nsrc > fdtd::kMaxSources)
+    return fail(h, FDTD_ERR_INVALID_ARG, "nsrc must be 0..%d", fdtd::kMaxSources);
+  if (nsrc > 0 && (!sources || !waveforms || T_wave <= 0))
+    return fail(h, FDTD_ERR_INVALID_ARG, "sources need a waveform table");
+  DeviceGuard dg(h->desc.device);
+  for (int n = 0; n < nsrc; ++n) {
+    const fdtd_source& s = sources[n];
+    if (s.component < 0 || s.component > 5)
+      return fail(h, FDTD_ERR_INVALID_ARG, "source %d: bad component %d", n, s.component);
+    if (s.kind != FDTD_SRC_POINT && s.kind != FDTD_SRC_PLANE_Z)
+      return fail(h, FDTD_ERR_INVALID_ARG, "source %d: bad kind %d", n, s.kind);
+    if (s.k < 0 || s.k >= h->g.nz ||
+        (s.kind == FDTD_SRC_POINT && (s.i < 0 || s.i >= h->g.nx || s.j < 0 || s.j >= h->g.ny)))
+      return fail(h, FDTD_ERR_INVALID_ARG, "source %d outside the grid", n);
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  cudaFree(h->d_wave);
+  h->d_wave = nullptr;
+  h->nsrc = 0;
+  h->tw = 0;
+  if (nsrc > 0) {
+    const size_t bytes = (size_t)nsrc * T_wave * sizeof(float);
+    CUDA_TRY(h, cudaMalloc(&h->d_wave, bytes));
+    CUDA_TRY(h, cudaMemcpy(h->d_wave, waveforms, bytes, cudaMemcpyHostToDevice));
+  }
+  for (int n = 0; n < nsrc; ++n) {
+    h->src[n].comp = sources[n].component;
+    h->src[n].kind = sources[n].kind;
+    h->src[n].i = (int)sources[n].i;
+    h->src[n].j = (int)sources[n].j;
+    h->src[n].k = (int)sources[n].k;
+  }
+  h->nsrc = nsrc;
+  h->tw = T_wave;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_add_dft_monitor(fdtd_handle* h, int32_t component, int64_t k,
+                                 const double* freqs, int32_t nf, double scale, double dt,
+                                 int32_t* monitor_id) {
+  if (!h) return FDTD_ERR_INVALID_ARG;
+  if (h->nmon >= fdtd::kMaxMonitors)
+    return fail(h, FDTD_ERR_UNSUPPORTED, "at most %d monitors", fdtd::kMaxMonitors);
+  if (component < 0 || component > 5) return fail(h, FDTD_ERR_INVALID_ARG, "bad component");
+  if (k < 0 || k >= h->g.nz) return fail(h, FDTD_ERR_INVALID_ARG, "monitor plane outside grid");
+  if (!freqs || nf < 1 || nf > fdtd::kMaxFreqs)
+    return fail(h, FDTD_ERR_INVALID_ARG, "nf must be 1..%d", fdtd::kMaxFreqs);
+  DeviceGuard dg(h->desc.device);
+  MonitorHost& m = h->mon[h->nmon];
+  m = MonitorHost();
+  m.comp = component;
+  m.k = k;
+  m.nf = nf;
+  m.scale = scale;
+  m.dt = dt;
+  m.freqs.assign(freqs, freqs + nf);
+  const size_t bytes = (size_t)nf * h->g.nx * h->g.ny * sizeof(double);
+  CUDA_TRY(h, cudaMalloc(&m.re, bytes));
+  CUDA_TRY(h, cudaMalloc(&m.im, bytes));
+  CUDA_TRY(h, cudaMemsetAsync(m.re, 0, bytes, h->stream));
+  CUDA_TRY(h, cudaMemsetAsync(m.im, 0, bytes, h->stream));
+  if (monitor_id) *monitor_id = h->nmon;
+  h->nmon += 1;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_reset(fdtd_handle* h) {
+  if (!h) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  for (int s = 0; s < 2; ++s)
+    for (int c = 0; c < 6; ++c)
+      CUDA_TRY(h, cudaMemsetAsync(h->F[s][c], 0, h->cells * sizeof(float), h->stream));
+  for (int m = 0; m < h->nmon; ++m) {
+    const size_t bytes = (size_t)h->mon[m].nf * h->g.nx * h->g.ny * sizeof(double);
+    CUDA_TRY(h, cudaMemsetAsync(h->mon[m].re, 0, bytes, h->stream));
+    CUDA_TRY(h, cudaMemsetAsync(h->mon[m].im, 0, bytes, h->stream));
+  }
+  h->t = 0;
+  h->cur = 0;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
+  if (!h || T < 0) return FDTD_ERR_INVALID_ARG;
+  if (h->coef_mode == kCoefNone)
+    return fail(h, FDTD_ERR_INVALID_ARG, "coefficients are not set");
+  if (T == 0) return FDTD_OK;
+  DeviceGuard dg(h->desc.device);
+  cudaStream_t st = pick_stream(h, stream);
+  if (st != h->stream) {
+    // Order the caller's stream after any work queued on the handle's own stream.
+    cudaEvent_t ev;
+    CUDA_TRY(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventRecord(ev, h->stream));
+    CUDA_TRY(h, cudaStreamWaitEvent(st, ev, 0));
+    cudaEventDestroy(ev);
+  }
+  fdtd_status s = ensure_tables(h, h->t + T);
+  if (s != FDTD_OK) return s;
+  int kernel = h->desc.kernel;
+  if (kernel == FDTD_KERNEL_AUTO)
+    kernel = h->coef_mode == kCoefMaterial ? FDTD_KERNEL_TILED : FDTD_KERNEL_NAIVE;
+  if (kernel == FDTD_KERNEL_TILED && h->coef_mode != kCoefMaterial)
+    return fail(h, FDTD_ERR_UNSUPPORTED,
+                "the tiled kernel needs a material map (more than %d distinct coefficient "
+                "tuples were given)", kMaxMaterials);
+  int launches = 0;
+  const fdtd::Sources S = make_sources(h);
+  const fdtd::Monitors M = make_monitors(h);
+  if (kernel == FDTD_KERNEL_NAIVE) {
+    fdtd::FieldPtrs F;
+    for (int c = 0; c < 6; ++c) F.f[c] = h->F[h->cur][c];
+    const bool matm = h->coef_mode == kCoefMaterial;
+    for (int64_t n = 0; n < T; ++n) {
+      CUDA_TRY(h, fdtd::launch_naive_step(h->g, F, matm ? nullptr : h->coef, matm ? h->mat : nullptr,
+                                          h->table, S, M, h->t, h->desc.dx, st, &launches));
+      h->t += 1;
+    }
+    h->last_kernel = FDTD_KERNEL_NAIVE;
+  } else {
+    if (!h->cfg_ready) {
+      s = autotune(h, st);
+      if (s != FDTD_OK) return s;
+    }
+    fdtd::TiledConfig c = h->cfg;
+    s = ensure_maps(h, c.rows);
+    if (s != FDTD_OK) return s;
+    int64_t left = T;
+    while (left > 0) {
+      fdtd::TiledConfig cc = c;
+      if (left < c.blt) cc.blt = (int)left;
+      if ((h->g.nz + cc.z_chunks - 1) / cc.z_chunks < 2 * cc.blt) cc.z_chunks = 1;
+      const fdtd::TiledArgs a = make_tiled_args(h, cc, h->t, true);
+      CUDA_TRY(h, fdtd::launch_tiled(cc, a, h->g, st));
+      ++launches;
+      h->cur ^= 1;
+      h->t += cc.blt;
+      left -= cc.blt;
+    }
+    h->last_kernel = FDTD_KERNEL_TILED;
+  }
+  h->last_launches = launches;
+  if (st != h->stream) {
+    cudaEvent_t ev;
+    CUDA_TRY(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventRecord(ev, st));
+    CUDA_TRY(h, cudaStreamWaitEvent(h->stream, ev, 0));
+    cudaEventDestroy(ev);
+  }
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_sync(fdtd_handle* h) {
+  if (!h) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return check_device_error(h);
+}
+
+fdtd_status fdtd_get_step(const fdtd_handle* h, int64_t* t) {
+  if (!h || !t) return FDTD_ERR_INVALID_ARG;
+  *t = h->t;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_get_field(fdtd_handle* h, int32_t component, float* host_out) {
+  if (!h || !host_out || component < 0 || component > 5) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  CUDA_TRY(h, cudaMemcpy2DAsync(host_out, (size_t)h->g.nx * 4, h->F[h->cur][component],
+                                (size_t)h->g.pitch * 4, (size_t)h->g.nx * 4,
+                                (size_t)h->g.ny * h->g.nz, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return check_device_error(h);
+}
+
+fdtd_status fdtd_get_field_device(fdtd_handle* h, int32_t component, float* dev_out,
+                                  void* stream) {
+  if (!h || !dev_out || component < 0 || component > 5) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  CUDA_TRY(h, cudaMemcpy2DAsync(dev_out, (size_t)h->g.nx * 4, h->F[h->cur][component],
+                                (size_t)h->g.pitch * 4, (size_t)h->g.nx * 4,
+                                (size_t)h->g.ny * h->g.nz, cudaMemcpyDeviceToDevice,
+                                pick_stream(h, stream)));
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_set_field(fdtd_handle* h, int32_t component, const float* host_in) {
+  if (!h || !host_in || component < 0 || component > 5) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  CUDA_TRY(h, cudaMemcpy2DAsync(h->F[h->cur][component], (size_t)h->g.pitch * 4, host_in,
+                                (size_t)h->g.nx * 4, (size_t)h->g.nx * 4,
+                                (size_t)h->g.ny * h->g.nz, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_get_dft(fdtd_handle* h, int32_t monitor_id, double* re, double* im) {
+  if (!h || monitor_id < 0 || monitor_id >= h->nmon || !re || !im) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  const MonitorHost& m = h->mon[monitor_id];
+  const size_t bytes = (size_t)m.nf * h->g.nx * h->g.ny * sizeof(double);
+  CUDA_TRY(h, cudaMemcpyAsync(re, m.re, bytes, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(im, m.im, bytes, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return check_device_error(h);
+}
+
+fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6) {
+  if (!h || !scale6) return FDTD_ERR_INVALID_ARG;
+  if (h->desc.storage == FDTD_STORE_F32) return FDTD_OK;
+  return fail(h, FDTD_ERR_UNSUPPORTED, "reduced-precision storage is not built");
+}
+
+fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out5) {
+  if (!h || !out5) return FDTD_ERR_INVALID_ARG;
+  out5[0] = h->last_kernel;
+  out5[1] = h->cfg.blt;
+  out5[2] = h->cfg.rows;
+  out5[3] = h->cfg.z_chunks;
+  out5[4] = h->last_launches;
+  return FDTD_OK;
+}
+
+}  // extern "C"

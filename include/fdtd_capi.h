@@ -1,0 +1,159 @@
+/* fdtd_capi.h -- C-ABI of the B200 FDTD (Yee) solver (libgdiamond_b200.so).
+ *
+ * The drop-in boundary for gDiamond's GPU update path.  In the reference every GPU variant is
+ * a member function of the header-only class gdiamond::gDiamond that allocates device memory,
+ * copies the 12 coefficient arrays in, runs T steps and copies the 6 fields out, all on the
+ * legacy default stream (e.g. update_FDTD_gpu_2D, gDiamond/gdiamond_gpu.cuh:483-648;
+ * update_FDTD_gpu_3D_warp_underutilization_fix, gDiamond/gdiamond_gpu.cuh:809-950;
+ * update_FDTD_mix_mapping_gpu_ver3, gDiamond/gdiamond_gpu_mm_ver3.cuh:478-740).  Here the same
+ * work is split into plain C calls on an opaque handle that keeps device state between calls;
+ * include/gdiamond_compat.hpp rebuilds the reference class surface on top of them.
+ *
+ * Conventions
+ *  - Grid layout on the host: x-fastest structure of arrays, idx = i + j*Nx + k*Nx*Ny, FP32.
+ *  - Field components: FDTD_EX..FDTD_HZ.  Coefficient arrays (12, in this order):
+ *    Cax Cay Caz Cbx Cby Cbz Dax Day Daz Dbx Dby Dbz  (gDiamond/gdiamond.hpp:891-904).
+ *  - One step = the E update of all interior cells followed by the H update of all interior
+ *    cells (gDiamond/gdiamond.hpp:1193-1221).  Cells on the six outer faces are never updated
+ *    (they keep their value, zero unless set), as in every reference path.
+ *  - Calls return fdtd_status and never exit or trap.  fdtd_last_error() gives the reason.
+ *  - A handle is not thread-safe; distinct handles are independent.
+ *  - fdtd_step is asynchronous on the given stream; fdtd_get_* synchronise.
+ */
+#ifndef GDIAMOND_B200_FDTD_CAPI_H
+#define GDIAMOND_B200_FDTD_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fdtd_handle fdtd_handle;
+
+typedef enum fdtd_status {
+  FDTD_OK = 0,
+  FDTD_ERR_INVALID_ARG = 1,
+  FDTD_ERR_OOM = 2,
+  FDTD_ERR_CUDA = 3,
+  FDTD_ERR_UNSUPPORTED = 4,
+  FDTD_ERR_DEVICE_TIMEOUT = 5,
+  FDTD_ERR_NUMERIC = 6
+} fdtd_status;
+
+typedef enum fdtd_component {
+  FDTD_EX = 0, FDTD_EY = 1, FDTD_EZ = 2, FDTD_HX = 3, FDTD_HY = 4, FDTD_HZ = 5
+} fdtd_component;
+
+/* Current-source components: J enters the E update as -J*dx, M the H update as -M*dx
+ * (gDiamond/gdiamond.hpp:1198-1218). */
+typedef enum fdtd_source_component {
+  FDTD_JX = 0, FDTD_JY = 1, FDTD_JZ = 2, FDTD_MX = 3, FDTD_MY = 4, FDTD_MZ = 5
+} fdtd_source_component;
+
+typedef enum fdtd_source_kind {
+  FDTD_SRC_POINT = 0,   /* one cell (i, j, k) */
+  FDTD_SRC_PLANE_Z = 1  /* every interior cell of the z-plane k (a current sheet) */
+} fdtd_source_kind;
+
+/* Kernel families.  AUTO picks TILED when the coefficients compress to a material table,
+ * else NAIVE. */
+typedef enum fdtd_kernel {
+  FDTD_KERNEL_AUTO = 0,
+  FDTD_KERNEL_NAIVE = 1,  /* one thread per cell, separate E and H launches per step */
+  FDTD_KERNEL_TILED = 2   /* z-streaming temporally tiled kernel, BLT steps per launch */
+} fdtd_kernel;
+
+/* Field storage in HBM.  Arithmetic is FP32 in every case; F16/BF16 store each component
+ * with a per-component scale (value = stored * scale). */
+typedef enum fdtd_storage {
+  FDTD_STORE_F32 = 0,
+  FDTD_STORE_F16 = 1,
+  FDTD_STORE_BF16 = 2
+} fdtd_storage;
+
+typedef struct fdtd_desc {
+  int64_t nx, ny, nz;   /* grid cells per axis, each >= 3 */
+  float dx;             /* spacing used in the -J*dx / -M*dx source terms */
+  int32_t device;       /* CUDA device ordinal */
+  int32_t storage;      /* fdtd_storage */
+  int32_t kernel;       /* fdtd_kernel */
+  int32_t blt;          /* time steps per tiled launch; 0 = autotuned */
+  int32_t tile_rows;    /* tiled-kernel rows per tile (8, 16 or 32); 0 = autotuned */
+  int32_t z_chunks;     /* tiled-kernel z-chunks per column; 0 = autotuned */
+} fdtd_desc;
+
+typedef struct fdtd_source {
+  int32_t component;    /* fdtd_source_component */
+  int32_t kind;         /* fdtd_source_kind */
+  int64_t i, j, k;      /* cell (point) or plane index k (plane) */
+} fdtd_source;
+
+/* Library version string. */
+const char* fdtd_version(void);
+const char* fdtd_status_string(fdtd_status s);
+/* Last error message of a handle (or of the last failed fdtd_create when h == NULL). */
+const char* fdtd_last_error(const fdtd_handle* h);
+
+/* Allocates device state for one grid: two field sets, zeroed (replaces the cudaMalloc /
+ * cudaMemset block of gDiamond/gdiamond_gpu.cuh:492-543). */
+fdtd_status fdtd_create(const fdtd_desc* desc, fdtd_handle** out);
+fdtd_status fdtd_destroy(fdtd_handle* h);
+
+/* Per-cell coefficients from 12 host arrays of Nx*Ny*Nz floats (the H2D copies of
+ * gDiamond/gdiamond_gpu.cuh:548-559).  The device deduplicates them into a material map
+ * (uint16 per cell) plus a coefficient table when at most 65536 distinct 12-tuples occur;
+ * otherwise the per-cell arrays are kept and the naive kernel is used. */
+fdtd_status fdtd_set_coefficients(fdtd_handle* h, const float* const* coef12);
+/* Same, from 12 device arrays already resident in HBM (unpitched, Nx*Ny*Nz floats each). */
+fdtd_status fdtd_set_coefficients_device(fdtd_handle* h, const float* const* coef12_dev);
+/* Number of distinct materials found (0 when the per-cell arrays are in use). */
+fdtd_status fdtd_material_count(const fdtd_handle* h, int32_t* nmat);
+
+/* Replaces the source list.  waveforms = nsrc rows of T_wave FP32 samples; sample t drives
+ * step t of the run (replaces the per-step 4-byte cudaMemcpy of the source value,
+ * gDiamond/gdiamond_gpu.cuh:568-570).  Steps t >= T_wave see zero.  At most 8 sources. */
+fdtd_status fdtd_set_sources(fdtd_handle* h, const fdtd_source* sources, int32_t nsrc,
+                             const float* waveforms, int64_t T_wave);
+
+/* Adds a running-DFT monitor on the z-plane k of one field component (the reference's
+ * update_field_FFT_xy, gDiamond/kernels.cuh:87-113, here with FP64 sums): after each step t
+ *   re[f][j][i] += (F(i,j,k) * cos(ph)) * scale,  im[f][j][i] -= (F(i,j,k) * sin(ph)) * scale,
+ *   ph = (2*pi*freqs[f]) * ((double)t * dt).
+ * At most 4 monitors, 64 frequencies each.  Writes the monitor id. */
+fdtd_status fdtd_add_dft_monitor(fdtd_handle* h, int32_t component, int64_t k,
+                                 const double* freqs, int32_t nf, double scale, double dt,
+                                 int32_t* monitor_id);
+
+/* Zeroes the fields and the monitor sums and sets the step counter to 0. */
+fdtd_status fdtd_reset(fdtd_handle* h);
+/* Runs T steps (asynchronous).  stream = a cudaStream_t, or NULL for the handle's stream. */
+fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream);
+/* Waits for the handle's work and reports any device-side error (e.g. a bounded wait that
+ * gave up, FDTD_ERR_DEVICE_TIMEOUT). */
+fdtd_status fdtd_sync(fdtd_handle* h);
+/* Global step counter (number of steps run since create/reset). */
+fdtd_status fdtd_get_step(const fdtd_handle* h, int64_t* t);
+
+/* Field and monitor transfer (synchronous).  Host arrays are Nx*Ny*Nz floats (fields) and
+ * nf*Nx*Ny doubles (monitor re/im, [f][j][i]). */
+fdtd_status fdtd_get_field(fdtd_handle* h, int32_t component, float* host_out);
+fdtd_status fdtd_set_field(fdtd_handle* h, int32_t component, const float* host_in);
+fdtd_status fdtd_get_dft(fdtd_handle* h, int32_t monitor_id, double* re, double* im);
+/* Device-to-device field copy into an unpitched Nx*Ny*Nz float array (asynchronous). */
+fdtd_status fdtd_get_field_device(fdtd_handle* h, int32_t component, float* dev_out,
+                                  void* stream);
+
+/* Per-component storage scale for F16/BF16 storage (ignored for F32); default 1. */
+fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6);
+
+/* Kernel configuration actually used by the last fdtd_step: out = {kernel, blt, tile_rows,
+ * z_chunks, launches in the last fdtd_step}. */
+fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out5);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,249 @@
+"""GPU parity: the CUDA kernels, called through the C-ABI, against the oracle (needs a GPU).
+
+The bar is bit-exactness: every multiply and add in the kernels is separately rounded, as in
+the reference's CPU build, so fields and FP64 monitor sums must equal the oracle's bit for bit.
+The north-star tolerance (relative L2 <= 1e-5 per component) is asserted as well, so a
+failure reports both.  Cases:
+  * the reference unit test (unittests/checker_gpu.cu): 100^3, 100 steps, the reference
+    constructor's coefficients and its Mz source -> the golden SHA-256 of update_FDTD_seq;
+  * the vacuum 100^3 Gaussian-Jz workload, 100 steps;
+  * every tiled (BLT, rows, z-chunks) instance on an odd grid with PML coefficients and J/M
+    point sources; plane sources with random permittivity; FP64 DFT monitors;
+  * per-cell coefficients that do not compress (naive fallback; tiled refused);
+  * at the full 256^3 x 1000 benchmark size: tiled == naive bit for bit, and linearity
+    (doubling the source doubles every field exactly);
+  * state handling: split step calls, reset, set_field.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import gdiamond_b200 as gd
+from gdiamond_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+REL_L2_TOL = 1e-5  # north-star FP32 tolerance (relative L2 per component)
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / nb if nb > 0 else np.linalg.norm(a - b)
+
+
+def assert_fields_match(F, F_ref, label=""):
+    for c in range(6):
+        assert rel_l2(F[c], F_ref[c]) <= REL_L2_TOL, f"{label} {oracle.COMPONENTS[c]} rel-L2"
+        assert np.array_equal(np.asarray(F[c], np.float32).view(np.uint32),
+                              np.asarray(F_ref[c], np.float32).view(np.uint32)), \
+            f"{label} {oracle.COMPONENTS[c]} not bit-identical"
+
+
+def gpu_run(shape, coefs, T, sources=(), monitors=(), kernel="auto", **kw):
+    sim = gd.Simulation(*shape, kernel=kernel, **kw)
+    sim.set_coefficients(coefs)
+    if sources:
+        sim.set_sources(sources)
+    mids = [sim.add_dft_monitor(m["component"], m["k"], m["freqs"], m.get("scale", 1.0))
+            for m in monitors]
+    sim.step(T)
+    sim.sync()
+    F = sim.fields()
+    D = [sim.get_dft(m) for m in mids]
+    cfg = sim.config()
+    sim.close()
+    return F, D, cfg
+
+
+def osrc(s):
+    return oracle.Source(s["component"], s["wave"], i=s.get("i", 0), j=s.get("j", 0), k=s["k"],
+                         kind=s.get("kind", 0))
+
+
+@pytest.mark.parametrize("kernel", ["naive", "tiled"])
+def test_reference_unit_test_100cube(kernel):
+    """unittests/checker_gpu.cu: seq vs GPU at 100^3 x 100 -- here against the golden seq."""
+    g = json.load(open(os.path.join(GOLDEN, "ref_100cube_T100.json")))
+    shape, T = tuple(g["shape"]), g["T"]
+    nx, ny, nz = shape
+    src = g["source_idx"]
+    coefs = W.reference_coefficients(shape)
+    sources = [dict(component="Mz", wave=W.reference_mz_wave(T), i=src % nx,
+                    j=(src // nx) % ny, k=src // (nx * ny))]
+    F, _, cfg = gpu_run(shape, coefs, T, sources, kernel=kernel)
+    assert cfg["kernel"] == kernel
+    for c, n in enumerate(oracle.COMPONENTS):
+        assert np.linalg.norm(F[c].astype(np.float64)) == pytest.approx(g["seq"][n]["l2"], rel=1e-5)
+        assert sha(F[c]) == g["seq"][n]["sha256"], n
+
+
+def test_vacuum_gaussian_jz_100cube():
+    shape, T = (100, 100, 100), 100
+    coefs = W.vacuum_coefficients(shape)
+    sources = [dict(component="Jz", wave=W.gaussian_wave(T), i=50, j=50, k=50)]
+    F_ref = oracle.run(shape, coefs, T, sources=[osrc(s) for s in sources])
+    for kernel in ("naive", "tiled"):
+        F, _, _ = gpu_run(shape, coefs, T, sources, kernel=kernel)
+        assert_fields_match(F, F_ref, kernel)
+
+
+CONFIGS = [(b, r, z) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)), (32, (1, 2, 4, 6)))
+           for b in bs for z in (1, 3)]
+
+
+@pytest.mark.parametrize("blt,rows,zc", CONFIGS)
+def test_tiled_instances_pml_point_sources(blt, rows, zc):
+    shape, T = (45, 37, 29), 13
+    coefs = W.reference_coefficients(shape)
+    w = W.gaussian_wave(T, delay=4.0, width=2.0, period=5.0)
+    sources = [dict(component="Jz", wave=w, i=22, j=18, k=14),
+               dict(component="Mx", wave=w * np.float32(0.5), i=3, j=30, k=20),
+               dict(component="Jy", wave=w, i=1, j=1, k=1)]
+    F_ref = oracle.run(shape, coefs, T, sources=[osrc(s) for s in sources])
+    F, _, cfg = gpu_run(shape, coefs, T, sources, kernel="tiled", blt=blt, tile_rows=rows,
+                        z_chunks=zc)
+    assert (cfg["blt"], cfg["tile_rows"], cfg["z_chunks"]) == (blt, rows, zc)
+    assert_fields_match(F, F_ref, f"blt={blt} rows={rows} zc={zc}")
+
+
+@pytest.mark.parametrize("kernel", ["naive", "tiled"])
+def test_plane_source_random_eps_and_monitors(kernel):
+    shape, T = (64, 48, 40), 60
+    nx, ny, nz = shape
+    rng = np.random.default_rng(7)
+    eps = W.spheres_eps(shape, n_spheres=12, r_range=(3, 9), seed=11)
+    coefs = W.reference_coefficients(shape, eps_re=eps)
+    w = W.gaussian_wave(T, delay=20.0, width=6.0, period=10.0)
+    sources = [dict(component="Jz", wave=w, k=12, kind=gd.SRC_PLANE_Z),
+               dict(component="My", wave=w, i=30, j=20, k=25)]
+    freqs = W.source_band(5, period=10.0, width=6.0)
+    mons = [dict(component="Ez", k=30, freqs=freqs, scale=50.0 / T),
+            dict(component="Hx", k=8, freqs=freqs[:3], scale=1.0)]
+    omons = [oracle.Monitor(m["component"], m["k"], m["freqs"], m["scale"]) for m in mons]
+    F_ref = oracle.run(shape, coefs, T, sources=[osrc(s) for s in sources], monitors=omons)
+    F, D, _ = gpu_run(shape, coefs, T, sources, mons, kernel=kernel)
+    assert_fields_match(F, F_ref, kernel)
+    for (re, im), om in zip(D, omons):
+        assert np.abs(om.re).max() > 0
+        assert np.array_equal(re, om.re) and np.array_equal(im, om.im)
+    del rng
+
+
+def test_per_cell_coefficients_fall_back_to_naive():
+    shape, T = (48, 40, 44), 20  # 84480 cells, almost all with their own 12-tuple (> 65536)
+    n = int(np.prod(shape))
+    rng = np.random.default_rng(3)
+    coefs = [c.copy() for c in W.vacuum_coefficients(shape)]
+    coefs[0] = rng.uniform(0.9, 1.0, n).astype(np.float32)  # lossy Cax, distinct per cell
+    sources = [dict(component="Jz", wave=W.gaussian_wave(T, delay=8, width=3, period=6),
+                    i=24, j=20, k=22)]
+    F_ref = oracle.run(shape, coefs, T, sources=[osrc(s) for s in sources])
+    F, _, cfg = gpu_run(shape, coefs, T, sources, kernel="auto")
+    assert cfg["kernel"] == "naive"
+    assert_fields_match(F, F_ref, "per-cell")
+    sim = gd.Simulation(*shape, kernel="tiled")
+    sim.set_coefficients(coefs)
+    assert sim.material_count() == 0
+    with pytest.raises(gd.FdtdError) as e:
+        sim.step(2)
+    assert e.value.status == 4  # FDTD_ERR_UNSUPPORTED
+    sim.close()
+
+
+def test_material_count_of_reference_constructor():
+    sim = gd.Simulation(60, 50, 40)
+    sim.set_coefficients(W.reference_coefficients((60, 50, 40)))
+    n = sim.material_count()
+    coefs = W.reference_coefficients((60, 50, 40))
+    stacked = np.stack([c.view(np.uint32) for c in coefs], 1)
+    assert n == len(np.unique(stacked, axis=0))
+    sim.close()
+
+
+def test_full_size_tiled_equals_naive_and_is_linear():
+    """256^3 x 1000 (the benchmark workload): size-independent properties."""
+    shape, T = (256, 256, 256), 1000
+    coefs = W.vacuum_coefficients(shape)
+    w = W.gaussian_wave(T)
+    freqs = W.source_band(8)
+    mons = [dict(component="Ez", k=128, freqs=freqs, scale=1.0)]
+    src = [dict(component="Jz", wave=w, i=128, j=128, k=128)]
+    Ft, Dt, cfg = gpu_run(shape, coefs, T, src, mons, kernel="tiled")
+    Fn, Dn, _ = gpu_run(shape, coefs, T, src, mons, kernel="naive")
+    for c in range(6):
+        assert np.array_equal(Ft[c].view(np.uint32), Fn[c].view(np.uint32)), oracle.COMPONENTS[c]
+    assert np.array_equal(Dt[0][0], Dn[0][0]) and np.array_equal(Dt[0][1], Dn[0][1])
+    assert np.abs(Dt[0][0]).max() > 0
+    src2 = [dict(component="Jz", wave=w * np.float32(2), i=128, j=128, k=128)]
+    F2, D2, _ = gpu_run(shape, coefs, T, src2, mons, kernel="tiled")
+    for c in range(6):
+        assert np.array_equal(F2[c], Ft[c] * np.float32(2)), oracle.COMPONENTS[c]
+    assert np.array_equal(D2[0][0], Dt[0][0] * 2)
+    assert np.isfinite(Ft[2]).all() and np.abs(Ft[2]).max() > 0
+
+
+def test_split_steps_reset_and_set_field():
+    shape = (33, 29, 31)
+    coefs = W.reference_coefficients(shape)
+    w = W.gaussian_wave(40, delay=10, width=4, period=8)
+    src = [dict(component="Jz", wave=w, i=16, j=14, k=15)]
+    rng = np.random.default_rng(5)
+    init = [rng.standard_normal(int(np.prod(shape))).astype(np.float32) for _ in range(6)]
+    F_ref = oracle.run(shape, coefs, 40, sources=[osrc(s) for s in src], fields=init)
+    sim = gd.Simulation(*shape, kernel="tiled", blt=4)
+    sim.set_coefficients(coefs)
+    sim.set_sources(src)
+    for c in range(6):
+        sim.set_field(c, init[c])
+    sim.step(7)
+    sim.step(13)
+    sim.step(20)
+    assert sim.t == 40
+    assert_fields_match(sim.fields(), F_ref, "split")
+    sim.reset()
+    assert sim.t == 0
+    assert all(np.count_nonzero(f) == 0 for f in sim.fields())
+    sim.close()
+
+
+def test_step_on_external_stream():
+    torch = pytest.importorskip("torch")
+    shape, T = (40, 40, 40), 30
+    coefs = W.vacuum_coefficients(shape)
+    src = [dict(component="Jz", wave=W.gaussian_wave(T, delay=10, width=4, period=8),
+                i=20, j=20, k=20)]
+    F_ref = oracle.run(shape, coefs, T, sources=[osrc(s) for s in src])
+    sim = gd.Simulation(*shape)
+    sim.set_coefficients(coefs)
+    sim.set_sources(src)
+    s = torch.cuda.Stream()
+    sim.step(T, stream=s)
+    s.synchronize()
+    assert_fields_match(sim.fields(), F_ref, "stream")
+    sim.close()
+
+
+def test_invalid_arguments_return_status():
+    sim = gd.Simulation(20, 20, 20)
+    with pytest.raises(gd.FdtdError) as e:
+        sim.step(1)  # coefficients not set
+    assert e.value.status == 1
+    with pytest.raises(gd.FdtdError):
+        sim.set_sources([dict(component="Jz", wave=np.ones(3, np.float32), i=25, j=1, k=1)])
+    for _ in range(4):
+        sim.add_dft_monitor("Ez", 10, [1.0])
+    with pytest.raises(gd.FdtdError) as e:
+        sim.add_dft_monitor("Ez", 10, [1.0])
+    assert e.value.status == 4
+    sim.close()
