@@ -38,7 +38,6 @@ sys.path.insert(0, ROOT)
 SHAPE = (256, 256, 256)
 T_STEPS = 1000
 N_FREQS = 8
-MON_K = 128
 B_ALG = 96  # algorithmic bytes per FP32 cell-update (6 fields r+w, 12 coefficients r)
 WORKLOAD = "fdtd3d_256cube_vacuum_gaussJz_T1000_dft8_zplane"
 METRIC = "Gcell-updates/s"
@@ -134,13 +133,14 @@ def traffic_from_profile(cfg):
 # ------------------------------------------------------------------ reference arm / CPU
 
 
-def cpu_reference_sample(target_s=8.0, max_T=64):
-    """Times the reference's update_FDTD_omp on the 256^3 grid for a bounded number of steps.
-    Returns (Gcell/s, cores, sample description, seconds, T)."""
+def cpu_reference_sample(target_s=12.0, max_T=400):
+    """Times the reference's update_FDTD_omp on the 256^3 grid for a bounded number of steps
+    (about target_s seconds).  Returns (Gcell/s, cores, T, seconds)."""
     import oracle
     r = oracle.Reference(*SHAPE)
-    t1 = r.run_omp(1)
-    T = int(max(1, min(max_T, target_s / max(t1, 1e-3))))
+    t2, t4 = r.run_omp(2), r.run_omp(4)
+    per_step = max((t4 - t2) / 2, 1e-4)  # the call's fixed cost (temporaries) cancels
+    T = int(max(2, min(max_T, target_s / per_step)))
     secs = r.run_omp(T)
     cores = oracle.ref().gdref_max_threads()
     r.close()
@@ -158,8 +158,9 @@ def run_reference_arm(args):
         return 0
     r = oracle.Reference(*SHAPE)
     cores = oracle.ref().gdref_max_threads()
-    t1 = r.run_omp(1)
-    T = int(max(1, min(64, 3.0 / max(t1, 1e-3))))  # each step a ~3 s bounded sample
+    t2, t4 = r.run_omp(2), r.run_omp(4)
+    per_step = max((t4 - t2) / 2, 1e-4)
+    T = int(max(2, min(200, 3.0 / per_step)))  # each bench step a ~3 s bounded sample
     for _ in range(args.warmup):
         r.run_omp(T)
     secs = [r.run_omp(T) for _ in range(args.steps)]
@@ -211,22 +212,25 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    nx, ny, nz = SHAPE
+    shape = tuple(int(v) for v in args.grid.split(","))
+    T_run = args.timesteps
+    nx, ny, nz = shape
     ncell = nx * ny * nz
-    coefs = W.vacuum_coefficients(SHAPE)
-    wave = W.gaussian_wave(T_STEPS)
+    coefs = W.vacuum_coefficients(shape)
+    wave = W.gaussian_wave(T_run)
     freqs = W.source_band(N_FREQS)
     src = [dict(component="Jz", wave=wave, i=nx // 2, j=ny // 2, k=nz // 2)]
 
-    sim = gd.Simulation(nx, ny, nz, device=local)
+    sim = gd.Simulation(nx, ny, nz, device=local, kernel=args.kernel, blt=args.blt,
+                        tile_rows=args.rows, z_chunks=args.zchunks)
     sim.set_coefficients(coefs)
     sim.set_sources(src)
-    mid = sim.add_dft_monitor("Ez", MON_K, freqs, scale=1.0)
+    mid = sim.add_dft_monitor("Ez", nz // 2, freqs, scale=1.0)
     stream = torch.cuda.Stream()
 
     def one_step():
         sim.reset()
-        sim.step(T_STEPS, stream=stream)
+        sim.step(T_run, stream=stream)
 
     # warm-up (the first step also runs the autotuner)
     for _ in range(max(args.warmup, 1)):
@@ -249,7 +253,7 @@ def run_ours(args):
     for k in range(args.steps):
         sim.reset()
         ev[k][0].record(stream)
-        sim.step(T_STEPS, stream=stream)
+        sim.step(T_run, stream=stream)
         ev[k][1].record(stream)
     t_end.record(stream)
     torch.cuda.synchronize()
@@ -259,7 +263,7 @@ def run_ours(args):
     total_ms = max_over_ranks(t_start.elapsed_time(t_end))
     kern_ms = [a.elapsed_time(b) for a, b in ev]
     ms_per_step = total_ms / args.steps
-    value = world * ncell * T_STEPS * args.steps / (total_ms / 1e3) / 1e9
+    value = world * ncell * T_run * args.steps / (total_ms / 1e3) / 1e9
     launch_ms = statistics.mean(kern_ms) / launches_per_step
 
     # ---------------- end to end through the C-ABI with host buffers
@@ -272,28 +276,31 @@ def run_ours(args):
     def e2e_step():
         sim.set_coefficients(pinned)
         sim.reset()
-        sim.step(T_STEPS)
+        sim.step(T_run)
         for c in range(6):
             sim.get_field(c, out=fields_out[c])
         return sim.get_dft(mid)
 
-    e2e_step()
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        re, im = e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = world * ncell * T_STEPS * args.steps / e2e_s / 1e9
-    h2d = 12 * ncell * 4 + wave.nbytes
-    d2h = 6 * ncell * 4 + re.nbytes + im.nbytes
+    e2e = None
+    if not args.no_e2e:
+        e2e_step()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            re, im = e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": world * ncell * T_run * args.steps / e2e_s / 1e9,
+               "unit": "Gcell-updates/s",
+               "h2d_bytes_per_step": 12 * ncell * 4 + wave.nbytes,
+               "d2h_bytes_per_step": 6 * ncell * 4 + re.nbytes + im.nbytes}
 
     # ---------------- roofline of the dominant kernel (the tiled kernel)
     hbm, kind = peaks()
     cells_per_launch = ncell * cfg["blt"]
     achieved = B_ALG * cells_per_launch / (launch_ms / 1e3) / 1e9
-    traffic = traffic_from_profile(cfg)
+    traffic = traffic_from_profile(cfg) if shape == SHAPE else None
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -316,7 +323,9 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded shapes of the workload; no dataset)",
-        "config": {"workload": WORKLOAD, "grid": list(SHAPE), "timesteps": T_STEPS,
+        "config": {"workload": WORKLOAD if (shape, T_run) == (SHAPE, T_STEPS) else
+                   f"fdtd3d_{nx}x{ny}x{nz}_vacuum_gaussJz_T{T_run}_dft8_zplane",
+                   "grid": list(shape), "timesteps": T_run,
                    "dft_freqs": N_FREQS, "kernel": cfg["kernel"], "blt": cfg["blt"],
                    "tile_rows": cfg["tile_rows"], "z_chunks": cfg["z_chunks"],
                    "parallelism": f"replicas{world}",
@@ -327,8 +336,7 @@ def run_ours(args):
                              f"per launch / mean launch time {launch_ms:.4f} ms; peak {kind}; "
                              f"temporal tiling lets frac exceed 1"},
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_value, "unit": "Gcell-updates/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+        "e2e": e2e,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
     }
@@ -343,6 +351,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer run")
+    ap.add_argument("--grid", default="256,256,256", help="NX,NY,NZ (profiling cases)")
+    ap.add_argument("--timesteps", type=int, default=T_STEPS)
+    ap.add_argument("--kernel", default="auto", choices=["auto", "naive", "tiled"])
+    ap.add_argument("--blt", type=int, default=0, help="force time steps per launch")
+    ap.add_argument("--rows", type=int, default=0, help="force tile rows")
+    ap.add_argument("--zchunks", type=int, default=0, help="force z-chunks")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -240,18 +240,18 @@ fdtd::TiledArgs make_tiled_args(fdtd_handle* h, const fdtd::TiledConfig& c, long
 // Candidate tiled configurations for the autotuner.
 std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
   std::vector<fdtd::TiledConfig> out;
-  const int blts[] = {1, 2, 3, 4, 5, 6};
-  const int rows_l[] = {8, 16, 32};
-  const int zc[] = {1, 2, 4, 8};
+  std::vector<int> blts = {1, 2, 3, 4, 5, 6}, rows_l = {8, 16, 32}, zc = {1, 2, 4, 8};
+  if (h->desc.blt > 0) blts = {h->desc.blt};
+  if (h->desc.tile_rows > 0) rows_l = {h->desc.tile_rows};
+  if (h->desc.z_chunks > 0) zc = {h->desc.z_chunks};
+  const bool forced_z = h->desc.z_chunks > 0;
   for (int rows : rows_l)
     for (int b : blts)
       for (int z : zc) {
         fdtd::TiledConfig c{b, rows, z};
         if (!fdtd::tiled_config_supported(c)) continue;
-        if (h->desc.blt > 0 && b != h->desc.blt) continue;
-        if (h->desc.tile_rows > 0 && rows != h->desc.tile_rows) continue;
-        if (h->desc.z_chunks > 0 && z != h->desc.z_chunks) continue;
-        if ((h->g.nz + z - 1) / z < 2 * b) continue;  // chunk shorter than its halo
+        // A chunk shorter than its 2*BLT warm-up is only worth it when asked for.
+        if (!forced_z && (h->g.nz + z - 1) / z < 2 * b) continue;
         out.push_back(c);
       }
   return out;
@@ -608,7 +608,6 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
     while (left > 0) {
       fdtd::TiledConfig cc = c;
       if (left < c.blt) cc.blt = (int)left;
-      if ((h->g.nz + cc.z_chunks - 1) / cc.z_chunks < 2 * cc.blt) cc.z_chunks = 1;
       const fdtd::TiledArgs a = make_tiled_args(h, cc, h->t, true);
       CUDA_TRY(h, fdtd::launch_tiled(cc, a, h->g, st));
       ++launches;

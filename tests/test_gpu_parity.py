@@ -187,9 +187,19 @@ def test_full_size_tiled_equals_naive_and_is_linear():
     assert np.abs(Dt[0][0]).max() > 0
     src2 = [dict(component="Jz", wave=w * np.float32(2), i=128, j=128, k=128)]
     F2, D2, _ = gpu_run(shape, coefs, T, src2, mons, kernel="tiled")
+    # Scaling every input by 2 scales every IEEE operation exactly except in the subnormal
+    # range (the far tail of the wavefront).  Once a bit differs the two runs round
+    # differently, so over 1000 steps of a closed (PEC) box they drift apart by the FP32
+    # rounding noise (~2e-6 relative): linearity holds to the FP32 tolerance.  Each
+    # component's difference is measured against its whole field vector (E or H): Hz of a Jz
+    # dipole in vacuum is zero by symmetry and holds only rounding noise.
     for c in range(6):
-        assert np.array_equal(F2[c], Ft[c] * np.float32(2)), oracle.COMPONENTS[c]
-    assert np.array_equal(D2[0][0], Dt[0][0] * 2)
+        grp = range(0, 3) if c < 3 else range(3, 6)
+        ref_norm = np.sqrt(sum(np.linalg.norm(2 * Ft[q].astype(np.float64)) ** 2 for q in grp))
+        err = np.linalg.norm(F2[c].astype(np.float64) - 2 * Ft[c].astype(np.float64))
+        assert err / ref_norm <= REL_L2_TOL, oracle.COMPONENTS[c]
+    assert rel_l2(D2[0][0], Dt[0][0] * 2) <= REL_L2_TOL
+    assert rel_l2(D2[0][1], Dt[0][1] * 2) <= REL_L2_TOL
     assert np.isfinite(Ft[2]).all() and np.abs(Ft[2]).max() > 0
 
 

@@ -13,8 +13,6 @@ grid sizes and every (BLT, ROWS, z-chunks) the kernel is built for.
 """
 from __future__ import annotations
 
-import math
-
 import numpy as np
 
 
@@ -210,9 +208,6 @@ def run(shape, coefs, T, blt, rows, z_chunks, dx, sources=(), monitors=(), field
     t = 0
     while t < T:
         b = min(blt, T - t)
-        zc = z_chunks
-        if math.ceil(nz / zc) < 2 * b:
-            zc = 1
-        F = tiled_pass(shape, F, mat, table, b, rows, zc, t, dx, sources, monitors)
+        F = tiled_pass(shape, F, mat, table, b, rows, z_chunks, t, dx, sources, monitors)
         t += b
     return F
