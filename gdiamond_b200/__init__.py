@@ -33,6 +33,7 @@ EXPORTS = (
     "fdtd_set_sources", "fdtd_add_dft_monitor", "fdtd_reset", "fdtd_step", "fdtd_sync",
     "fdtd_get_step", "fdtd_get_field", "fdtd_set_field", "fdtd_get_dft",
     "fdtd_get_field_device", "fdtd_set_storage_scale", "fdtd_get_config",
+    "fdtd_build_material_map_noalloc",
 )
 
 

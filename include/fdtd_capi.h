@@ -152,6 +152,27 @@ fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6);
  * z_chunks, launches in the last fdtd_step}. */
 fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out5);
 
+/* Builds a material map from 12 device coefficient arrays without allocating anything.
+ * No counterpart in the reference (which keeps 12 per-cell arrays); it is the allocation-free
+ * form of the deduplication that fdtd_set_coefficients runs, for callers that cannot allocate
+ * device memory at that point: an application that owns all device memory through its own
+ * pool, a loop where cudaMalloc's implicit synchronisation is not acceptable, or code that
+ * must not grow its footprint after start-up.
+ *   coef12_dev   12 device arrays of nx*ny*nz floats (unpitched, Cax..Dbz)
+ *   mat_dev      out: nx*ny*nz uint16 material ids (device)
+ *   table_dev    out: max_materials x 12 floats (device), row id = the tuple Cax..Dbz
+ *   nmat_out     out (host): number of distinct tuples found
+ * Limit: at most 4096 distinct tuples; max_materials > 4096 is rejected with
+ * FDTD_ERR_INVALID_ARG, data with more distinct tuples than max_materials with
+ * FDTD_ERR_UNSUPPORTED.  The scratch is a fixed ~1.25 MB device array that every GPU loading the
+ * library holds until exit; all calls share it (each clears it first), so calls that overlap
+ * on the GPU race.  The first call on each device resolves that array's address; make it
+ * before any stream capture.  The call synchronises `stream` (a cudaStream_t or NULL). */
+fdtd_status fdtd_build_material_map_noalloc(const float* const* coef12_dev, int64_t nx,
+                                            int64_t ny, int64_t nz, uint16_t* mat_dev,
+                                            float* table_dev, int32_t max_materials,
+                                            int32_t* nmat_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
