@@ -326,7 +326,8 @@ def run_ours(args):
         "config": {"workload": WORKLOAD if (shape, T_run) == (SHAPE, T_STEPS) else
                    f"fdtd3d_{nx}x{ny}x{nz}_vacuum_gaussJz_T{T_run}_dft8_zplane",
                    "grid": list(shape), "timesteps": T_run,
-                   "dft_freqs": N_FREQS, "kernel": cfg["kernel"], "blt": cfg["blt"],
+                   "dft_freqs": N_FREQS, "kernel": cfg["kernel"], "width": cfg.get("width"),
+                   "blt": cfg["blt"],
                    "tile_rows": cfg["tile_rows"], "z_chunks": cfg["z_chunks"],
                    "parallelism": f"replicas{world}",
                    "l2": "inputs (1.2 GB of fields) larger than L2; no flush"},
@@ -354,7 +355,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer run")
     ap.add_argument("--grid", default="256,256,256", help="NX,NY,NZ (profiling cases)")
     ap.add_argument("--timesteps", type=int, default=T_STEPS)
-    ap.add_argument("--kernel", default="auto", choices=["auto", "naive", "tiled"])
+    ap.add_argument("--kernel", default="auto",
+                    choices=["auto", "naive", "tiled", "tiled_w32", "tiled_w64"])
     ap.add_argument("--blt", type=int, default=0, help="force time steps per launch")
     ap.add_argument("--rows", type=int, default=0, help="force tile rows")
     ap.add_argument("--zchunks", type=int, default=0, help="force z-chunks")

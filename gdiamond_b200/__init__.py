@@ -22,7 +22,7 @@ LIB_PATH = os.path.join(_HERE, "libgdiamond_b200.so")
 COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 SOURCE_COMPONENTS = ("Jx", "Jy", "Jz", "Mx", "My", "Mz")
 COEFFS = ("Cax", "Cay", "Caz", "Cbx", "Cby", "Cbz", "Dax", "Day", "Daz", "Dbx", "Dby", "Dbz")
-KERNELS = {"auto": 0, "naive": 1, "tiled": 2}
+KERNELS = {"auto": 0, "naive": 1, "tiled": 2, "tiled_w32": 3, "tiled_w64": 4}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
 SRC_POINT, SRC_PLANE_Z = 0, 1
 
@@ -220,9 +220,10 @@ class Simulation:
     def config(self):
         out = (C.c_int32 * 5)()
         self._check(self._L.fdtd_get_config(self._h, out))
-        kernel = {1: "naive", 2: "tiled"}.get(out[0], "none")
-        return {"kernel": kernel, "blt": out[1], "tile_rows": out[2], "z_chunks": out[3],
-                "launches": out[4]}
+        kernel = {1: "naive", 3: "tiled", 4: "tiled"}.get(out[0], "none")
+        width = {3: 32, 4: 64}.get(out[0], 0)
+        return {"kernel": kernel, "width": width, "blt": out[1], "tile_rows": out[2],
+                "z_chunks": out[3], "launches": out[4]}
 
     # ---------------------------------------------------------------- results
     def get_field(self, component, out=None):

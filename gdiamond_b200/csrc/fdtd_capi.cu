@@ -91,7 +91,7 @@ struct fdtd_handle {
   bool cfg_ready = false;
   CUtensorMap maps[2][6];
   CUtensorMap mat_map;
-  int maps_rows = 0;
+  int maps_key = 0;  // width * 1000 + rows of the encoded boxes
   int last_kernel = 0, last_launches = 0;
   std::string err;
 };
@@ -151,19 +151,32 @@ fdtd_status encode_map(fdtd_handle* h, CUtensorMap* m, void* base, CUtensorMapDa
   return FDTD_OK;
 }
 
-fdtd_status ensure_maps(fdtd_handle* h, int rows) {
-  if (h->maps_rows == rows) return FDTD_OK;
+// Tensor maps of both field sets and of the material map for boxes {width, rows, 1} (fields)
+// and {width + 8, rows, 1} (material ids, widened so the box starts on an 8-element boundary).
+fdtd_status ensure_maps(fdtd_handle* h, int width, int rows) {
+  const int key = width * 1000 + rows;
+  if (h->maps_key == key) return FDTD_OK;
   for (int s = 0; s < 2; ++s)
     for (int c = 0; c < 6; ++c) {
       fdtd_status st = encode_map(h, &h->maps[s][c], h->F[s][c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                                  4, 32, rows);
+                                  4, width, rows);
       if (st != FDTD_OK) return st;
     }
+  const int mat_box = width == 64 ? fdtd::kMatBoxX2 : fdtd::kMatBoxX;
   fdtd_status st = encode_map(h, &h->mat_map, h->mat, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2,
-                              fdtd::kMatBoxX, rows);
+                              mat_box, rows);
   if (st != FDTD_OK) return st;
-  h->maps_rows = rows;
+  h->maps_key = key;
   return FDTD_OK;
+}
+
+cudaError_t launch_any(const fdtd::TiledConfig& c, const fdtd::TiledArgs& a, const Grid& g,
+                       cudaStream_t st) {
+  return c.width == 64 ? fdtd::launch_tiled2(c, a, g, st) : fdtd::launch_tiled(c, a, g, st);
+}
+
+bool config_supported(const fdtd::TiledConfig& c) {
+  return c.width == 64 ? fdtd::tiled2_config_supported(c) : fdtd::tiled_config_supported(c);
 }
 
 fdtd::Sources make_sources(const fdtd_handle* h) {
@@ -241,19 +254,23 @@ fdtd::TiledArgs make_tiled_args(fdtd_handle* h, const fdtd::TiledConfig& c, long
 std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
   std::vector<fdtd::TiledConfig> out;
   std::vector<int> blts = {1, 2, 3, 4, 5, 6}, rows_l = {8, 16, 32}, zc = {1, 2, 4, 8};
+  std::vector<int> widths = {32, 64};
   if (h->desc.blt > 0) blts = {h->desc.blt};
   if (h->desc.tile_rows > 0) rows_l = {h->desc.tile_rows};
   if (h->desc.z_chunks > 0) zc = {h->desc.z_chunks};
+  if (h->desc.kernel == FDTD_KERNEL_TILED_W32) widths = {32};
+  if (h->desc.kernel == FDTD_KERNEL_TILED_W64) widths = {64};
   const bool forced_z = h->desc.z_chunks > 0;
-  for (int rows : rows_l)
-    for (int b : blts)
-      for (int z : zc) {
-        fdtd::TiledConfig c{b, rows, z};
-        if (!fdtd::tiled_config_supported(c)) continue;
-        // A chunk shorter than its 2*BLT warm-up is only worth it when asked for.
-        if (!forced_z && (h->g.nz + z - 1) / z < 2 * b) continue;
-        out.push_back(c);
-      }
+  for (int w : widths)
+    for (int rows : rows_l)
+      for (int b : blts)
+        for (int z : zc) {
+          fdtd::TiledConfig c{b, rows, z, w};
+          if (!config_supported(c)) continue;
+          // A chunk shorter than its 2*BLT warm-up is only worth it when asked for.
+          if (!forced_z && (h->g.nz + z - 1) / z < 2 * b) continue;
+          out.push_back(c);
+        }
   return out;
 }
 
@@ -261,7 +278,8 @@ std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
 // and monitors off, so the simulation state is not changed) and keeps the fastest per step.
 fdtd_status autotune(fdtd_handle* h, cudaStream_t st) {
   const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz,
-                                   h->desc.blt * 10000 + h->desc.tile_rows * 100 + h->desc.z_chunks);
+                                   h->desc.kernel * 1000000 + h->desc.blt * 10000 +
+                                       h->desc.tile_rows * 100 + h->desc.z_chunks);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -281,21 +299,47 @@ fdtd_status autotune(fdtd_handle* h, cudaStream_t st) {
   cudaEvent_t e0, e1;
   CUDA_TRY(h, cudaEventCreate(&e0));
   CUDA_TRY(h, cudaEventCreate(&e1));
-  float best = 1e30f;
-  fdtd::TiledConfig best_c = cands[0];
-  const int reps = 2;
-  for (const auto& c : cands) {
-    fdtd_status s = ensure_maps(h, c.rows);
+  // Time one candidate: one untimed launch, then `reps` timed launches; ms per step.
+  auto time_cfg = [&](const fdtd::TiledConfig& c, int reps, float* per_step) -> fdtd_status {
+    fdtd_status s = ensure_maps(h, c.width, c.rows);
     if (s != FDTD_OK) return s;
     const fdtd::TiledArgs a = make_tiled_args(h, c, 0, false);
-    CUDA_TRY(h, fdtd::launch_tiled(c, a, h->g, st));  // warm-up
+    CUDA_TRY(h, launch_any(c, a, h->g, st));
     CUDA_TRY(h, cudaEventRecord(e0, st));
-    for (int r = 0; r < reps; ++r) CUDA_TRY(h, fdtd::launch_tiled(c, a, h->g, st));
+    for (int r = 0; r < reps; ++r) CUDA_TRY(h, launch_any(c, a, h->g, st));
     CUDA_TRY(h, cudaEventRecord(e1, st));
     CUDA_TRY(h, cudaEventSynchronize(e1));
     float ms = 0;
     CUDA_TRY(h, cudaEventElapsedTime(&ms, e0, e1));
-    const float per_step = ms / (reps * c.blt);
+    *per_step = ms / (reps * c.blt);
+    return FDTD_OK;
+  };
+  // Bring the SM clocks up before anything is compared (an idle GPU starts slow and would
+  // penalise whichever candidates run first): launch the first candidate for ~50 ms.
+  {
+    float warm = 0, spent = 0;
+    for (int r = 0; r < 64 && spent < 50.0f; ++r) {
+      fdtd_status s = time_cfg(cands[0], 2, &warm);
+      if (s != FDTD_OK) return s;
+      spent += warm * 2 * cands[0].blt;
+    }
+  }
+  std::vector<std::pair<float, size_t>> scored;
+  for (size_t i = 0; i < cands.size(); ++i) {
+    float per_step = 0;
+    fdtd_status s = time_cfg(cands[i], 3, &per_step);
+    if (s != FDTD_OK) return s;
+    scored.emplace_back(per_step, i);
+  }
+  // Re-time the best few with more launches and keep the fastest.
+  std::sort(scored.begin(), scored.end());
+  float best = 1e30f;
+  fdtd::TiledConfig best_c = cands[scored[0].second];
+  for (size_t r = 0; r < std::min<size_t>(4, scored.size()); ++r) {
+    const fdtd::TiledConfig& c = cands[scored[r].second];
+    float per_step = 0;
+    fdtd_status s = time_cfg(c, 8, &per_step);
+    if (s != FDTD_OK) return s;
     if (per_step < best) {
       best = per_step;
       best_c = c;
@@ -402,7 +446,7 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "grid axis too large");
   if (d->storage != FDTD_STORE_F32)
     return fail(nullptr, FDTD_ERR_UNSUPPORTED, "only FP32 field storage is built");
-  if (d->kernel < FDTD_KERNEL_AUTO || d->kernel > FDTD_KERNEL_TILED)
+  if (d->kernel < FDTD_KERNEL_AUTO || d->kernel > FDTD_KERNEL_TILED_W64)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "unknown kernel %d", d->kernel);
   if (d->blt < 0 || d->blt > 6) return fail(nullptr, FDTD_ERR_INVALID_ARG, "blt must be 0..6");
   if (d->tile_rows != 0 && d->tile_rows != 8 && d->tile_rows != 16 && d->tile_rows != 32)
@@ -579,7 +623,7 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
   int kernel = h->desc.kernel;
   if (kernel == FDTD_KERNEL_AUTO)
     kernel = h->coef_mode == kCoefMaterial ? FDTD_KERNEL_TILED : FDTD_KERNEL_NAIVE;
-  if (kernel == FDTD_KERNEL_TILED && h->coef_mode != kCoefMaterial)
+  if (kernel != FDTD_KERNEL_NAIVE && h->coef_mode != kCoefMaterial)
     return fail(h, FDTD_ERR_UNSUPPORTED,
                 "the tiled kernel needs a material map (more than %d distinct coefficient "
                 "tuples were given)", kMaxMaterials);
@@ -602,20 +646,20 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
       if (s != FDTD_OK) return s;
     }
     fdtd::TiledConfig c = h->cfg;
-    s = ensure_maps(h, c.rows);
+    s = ensure_maps(h, c.width, c.rows);
     if (s != FDTD_OK) return s;
     int64_t left = T;
     while (left > 0) {
       fdtd::TiledConfig cc = c;
       if (left < c.blt) cc.blt = (int)left;
       const fdtd::TiledArgs a = make_tiled_args(h, cc, h->t, true);
-      CUDA_TRY(h, fdtd::launch_tiled(cc, a, h->g, st));
+      CUDA_TRY(h, launch_any(cc, a, h->g, st));
       ++launches;
       h->cur ^= 1;
       h->t += cc.blt;
       left -= cc.blt;
     }
-    h->last_kernel = FDTD_KERNEL_TILED;
+    h->last_kernel = c.width == 64 ? FDTD_KERNEL_TILED_W64 : FDTD_KERNEL_TILED_W32;
   }
   h->last_launches = launches;
   if (st != h->stream) {

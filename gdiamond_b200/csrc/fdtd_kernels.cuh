@@ -18,8 +18,8 @@ cudaError_t launch_naive_step(const Grid& g, const FieldPtrs& F, const float* co
 
 // ---------------------------------------------------------------- tiled kernel
 struct TiledArgs {
-  CUtensorMap tm_src[6];  // 3-D maps of the source field set, box {32, rows, 1}
-  CUtensorMap tm_mat;     // 3-D map of the uint16 material map, box {40, rows, 1}
+  CUtensorMap tm_src[6];  // 3-D maps of the source field set, box {width, rows, 1}
+  CUtensorMap tm_mat;     // 3-D map of the uint16 material map, box {width + 8, rows, 1}
   Grid g;
   FieldPtrs dst;          // destination field set (pitched)
   const Material* table;
@@ -35,6 +35,7 @@ struct TiledConfig {
   int blt;        // time steps per launch
   int rows;       // tile rows (warps per CTA)
   int z_chunks;   // z-chunks per tile column
+  int width = 32; // cells per warp row: 32 (k_tiled.cu) or 64 (k_tiled2.cu, x-pairs)
 };
 
 // Tile geometry shared by the host (grid size, tensor-map boxes) and the kernel.
@@ -43,6 +44,15 @@ __host__ __device__ constexpr int tiled_xbase(int blt) { return -4 * ((blt + 3) 
 __host__ __device__ constexpr int tiled_sy(int blt, int rows) { return rows - 2 * blt; }
 constexpr int kTiledStages = 3;
 constexpr int kMatBoxX = 40;  // material box is widened to start on an 8-element boundary
+
+// Two-cells-per-thread family (k_tiled2.cu): 64-wide warp rows.
+__host__ __device__ constexpr int tiled2_sx(int blt) { return 4 * ((64 - 2 * blt) / 4); }
+constexpr int kTiled2Stages = 2;
+constexpr int kMatBoxX2 = 72;  // 64 + 4 alignment offset, rounded to a 16-byte row
+bool tiled2_config_supported(const TiledConfig& c);
+dim3 tiled2_grid(const TiledConfig& c, const Grid& g);
+cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& args, const Grid& g,
+                          cudaStream_t st);
 
 bool tiled_config_supported(const TiledConfig& c);
 size_t tiled_smem_bytes(const TiledConfig& c);

@@ -93,6 +93,21 @@ __global__ void __launch_bounds__(32 * TY) fdtd_tiled(const __grid_constant__ Ti
     const SourceDev& s = a.S.s[n];
     if ((s.kind == 0 && s.i == x && s.j == y) || (s.kind == 1 && col_int)) smask |= 1u << n;
   }
+  // CTA-uniform z-iteration ranges in which some level touches a source plane inside this tile
+  // or a monitor plane: E at plane p-s+1 and H at plane p-s for s = 1..B.  Outside them the
+  // per-level source and monitor code is skipped by every warp.
+  int src_lo = 1 << 30, src_hi = -(1 << 30), mon_lo = 1 << 30, mon_hi = -(1 << 30);
+  for (int n = 0; n < a.S.n; ++n) {
+    const SourceDev& s = a.S.s[n];
+    if (s.kind == 0 && (s.i < X || s.i >= X + 32 || s.j < Y || s.j >= Y + TY)) continue;
+    src_lo = min(src_lo, s.k);
+    src_hi = max(src_hi, s.k + B);
+  }
+  for (int n = 0; n < a.M.n; ++n) {
+    const int k = a.M.m[n].k + (a.M.m[n].comp < 3 ? 0 : 1);
+    mon_lo = min(mon_lo, k);
+    mon_hi = max(mon_hi, k + B - 1);
+  }
 
   if (tid == 0) {
     s_abort = 0;
@@ -144,6 +159,8 @@ __global__ void __launch_bounds__(32 * TY) fdtd_tiled(const __grid_constant__ Ti
       atomicExch(a.err, kErrTimeout);
     }
     if (B == 1) __syncthreads();  // orders last iteration's ebuf writes before this read
+    const bool src_iter = smask != 0 && p >= src_lo && p <= src_hi;
+    const bool mon_iter = p >= mon_lo && p <= mon_hi;
 
     const float* S0 = st_f + stage * 6 * K::PL;
 #pragma unroll
@@ -167,7 +184,7 @@ __global__ void __launch_bounds__(32 * TY) fdtd_tiled(const __grid_constant__ Ti
       float cz = sub(sub(Hc[1], hy_xm), sub(Hc[0], hx_ym));
       float En[3] = {Eo[0], Eo[1], Eo[2]};
       if (col_int && e >= 1 && e <= g.nz - 2) {
-        if (smask) {
+        if (src_iter) {
           float v;
           if (source_value(a.S, 0, x, y, e, t, &v)) cx = sub(cx, mul(v, dx));
           if (source_value(a.S, 1, x, y, e, t, &v)) cy = sub(cy, mul(v, dx));
@@ -189,7 +206,7 @@ __global__ void __launch_bounds__(32 * TY) fdtd_tiled(const __grid_constant__ Ti
       cz = sub(sub(ex_yp, Ep[s][0]), sub(ey_xp, Ep[s][1]));
       float Hn[3] = {Hp[s - 1][0], Hp[s - 1][1], Hp[s - 1][2]};
       if (col_int && e - 1 >= 1 && e - 1 <= g.nz - 2) {
-        if (smask) {
+        if (src_iter) {
           float v;
           if (source_value(a.S, 3, x, y, e - 1, t, &v)) cx = sub(cx, mul(v, dx));
           if (source_value(a.S, 4, x, y, e - 1, t, &v)) cy = sub(cy, mul(v, dx));
@@ -202,7 +219,7 @@ __global__ void __launch_bounds__(32 * TY) fdtd_tiled(const __grid_constant__ Ti
         Hn[2] = yee(mc.z, Hp[s - 1][2], mc.w, cz);
       }
       // ---------------- running DFT when this level passes a monitor plane
-      if (a.M.n && col_out) {
+      if (mon_iter && col_out) {
         for (int n = 0; n < a.M.n; ++n) {
           const MonitorDev& m = a.M.m[n];
           const int mk = m.comp < 3 ? e : e - 1;

@@ -1,0 +1,401 @@
+// k_tiled2.cu -- the z-streaming temporally tiled Yee kernel with two cells per thread in x.
+//
+// Same schedule as k_tiled.cu (TMA plane pipeline, BLT-level (z,t) wavefront, trapezoid tiles in
+// x and y, material map, fused FP64 DFT, bounded waits, bit-exact arithmetic), but each thread
+// owns an x-pair (2l, 2l+1) of a 64-wide warp row:
+//  * the pair's inner neighbours are in registers; only the pair edges cross lanes, so a level
+//    needs one shuffle per field direction per pair instead of per cell;
+//  * staged planes, y-exchange planes and outputs move as float2 (one shared/global instruction
+//    for two cells);
+//  * the x-trapezoid wastes 2*BLT of 64 columns instead of 2*BLT of 32;
+//  * monitor planes are tested once per z-iteration against a precomputed plane range.
+#include "fdtd_kernels.cuh"
+
+namespace fdtd {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr long long kWaitLimit = 2000000000LL;  // SM clocks, about one second
+
+template <int B, int TY>
+struct Tiled2 {
+  static constexpr int W = 64;                 // cells per warp row
+  static constexpr int PL = W * TY;            // elements of one staged field plane
+  static constexpr int MPL = kMatBoxX2 * TY;   // elements of one staged material plane
+  static constexpr int NS = kTiled2Stages;
+  static constexpr int SX = tiled2_sx(B);
+  static constexpr int SY = tiled_sy(B, TY);
+  static constexpr int XBASE = tiled_xbase(B);
+  static constexpr uint32_t STAGE_F_BYTES = 6u * PL * 4u;
+  static constexpr uint32_t STAGE_M_BYTES = MPL * 2u;
+  static constexpr uint32_t TX_BYTES = STAGE_F_BYTES + STAGE_M_BYTES;
+  static constexpr size_t OFF_M = (size_t)NS * STAGE_F_BYTES;
+  static constexpr size_t OFF_H = OFF_M + (size_t)NS * STAGE_M_BYTES;
+  static constexpr size_t OFF_E = OFF_H + 2u * 2u * PL * 4u;
+  static constexpr size_t OFF_BAR = OFF_E + (size_t)B * 2u * PL * 4u;
+  static constexpr size_t SMEM = OFF_BAR + NS * 8u + 128u;  // + alignment slack
+  static_assert(SY >= 1, "tile too short for this BLT");
+  static_assert(STAGE_M_BYTES % 128 == 0, "stage alignment");
+};
+
+struct Pair {
+  float a, b;  // even cell, odd cell
+};
+
+__device__ __forceinline__ float2 ld2(const float* p) { return *reinterpret_cast<const float2*>(p); }
+__device__ __forceinline__ void st2(float* p, float a, float b) {
+  *reinterpret_cast<float2*>(p) = make_float2(a, b);
+}
+
+template <int B, int TY>
+__global__ void __launch_bounds__(32 * TY) fdtd_tiled2(const __grid_constant__ TiledArgs a) {
+  using K = Tiled2<B, TY>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  float* st_f = reinterpret_cast<float*>(smem);
+  uint16_t* st_m = reinterpret_cast<uint16_t*>(smem + K::OFF_M);
+  float* hbuf = reinterpret_cast<float*>(smem + K::OFF_H);  // [2][Hz,Hx][PL]
+  float* ebuf = reinterpret_cast<float*>(smem + K::OFF_E);  // [B][Ex,Ez][PL]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + K::OFF_BAR);
+  __shared__ int s_abort;
+
+  const Grid g = a.g;
+  const int z0 = (int)blockIdx.z * a.zlen;
+  if (z0 >= g.nz) return;  // uniform across the CTA
+  const int z1 = min(g.nz, z0 + a.zlen);
+  const int ps = z0 - B;
+  const int niter = (z1 - z0) + 2 * B;
+
+  const int lx = threadIdx.x, ly = threadIdx.y;
+  const int tid = ly * 32 + lx;
+  const int X = (int)blockIdx.x * K::SX + K::XBASE;  // multiple of 4
+  const int Y = (int)blockIdx.y * K::SY - B;
+  const int X8 = X & ~7;
+  const int cx0 = 2 * lx;                            // tile column of the even cell
+  const int x0 = X + cx0, x1 = x0 + 1, y = Y + ly;
+  const bool row_int = y >= 1 && y <= g.ny - 2;
+  const bool int0 = row_int && x0 >= 1 && x0 <= g.nx - 2;
+  const bool int1 = row_int && x1 >= 1 && x1 <= g.nx - 2;
+  const bool row_out = ly >= B && ly < TY - B && y >= 0 && y < g.ny;
+  const bool out0 = row_out && cx0 >= B && cx0 < B + K::SX && x0 >= 0 && x0 < g.nx;
+  const bool out1 = row_out && cx0 + 1 >= B && cx0 + 1 < B + K::SX && x1 >= 0 && x1 < g.nx;
+  unsigned smask = 0;
+  for (int n = 0; n < a.S.n; ++n) {
+    const SourceDev& s = a.S.s[n];
+    const bool hit = s.kind == 0 ? (s.j == y && (s.i == x0 || s.i == x1)) : (int0 || int1);
+    if (hit) smask |= 1u << n;
+  }
+  // CTA-uniform z-iteration ranges in which some level touches a source plane inside this tile
+  // or a monitor plane: E at plane p-s+1 and H at plane p-s for s = 1..B.  Outside them the
+  // per-level source and monitor code is skipped by every warp.
+  int src_lo = 1 << 30, src_hi = -(1 << 30), mon_lo = 1 << 30, mon_hi = -(1 << 30);
+  for (int n = 0; n < a.S.n; ++n) {
+    const SourceDev& s = a.S.s[n];
+    if (s.kind == 0 && (s.i < X || s.i >= X + K::W || s.j < Y || s.j >= Y + TY)) continue;
+    src_lo = min(src_lo, s.k);
+    src_hi = max(src_hi, s.k + B);
+  }
+  for (int n = 0; n < a.M.n; ++n) {
+    const int k = a.M.m[n].k + (a.M.m[n].comp < 3 ? 0 : 1);  // E at p-s+1, H at p-s
+    mon_lo = min(mon_lo, k);
+    mon_hi = max(mon_hi, k + B - 1);
+  }
+
+  if (tid == 0) {
+    s_abort = 0;
+    for (int s = 0; s < K::NS; ++s) mbar_init(&bars[s], 1);
+    fence_mbar_init();
+  }
+  for (int q = tid; q < (4 + 2 * B) * K::PL; q += 32 * TY) hbuf[q] = 0.0f;
+  __syncthreads();
+
+  auto issue = [&](int it_) {
+    const int stage = it_ % K::NS;
+    uint64_t* bar = &bars[stage];
+    mbar_arrive_expect_tx(bar, K::TX_BYTES);
+    float* d = st_f + stage * 6 * K::PL;
+    const int pz = ps + it_;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) tma_load_3d(d + c * K::PL, &a.tm_src[c], bar, X, Y, pz);
+    tma_load_3d(st_m + stage * K::MPL, &a.tm_mat, bar, X8, Y, pz);
+  };
+  if (tid == 0) {
+    for (int it_ = 0; it_ < K::NS && it_ < niter; ++it_) issue(it_);
+  }
+
+  // Ep[s][c] / Hp[s][c]: level-s values of this thread's pair one iteration ago.
+  Pair Ep[B + 1][3], Hp[B + 1][3];
+#pragma unroll
+  for (int s = 0; s <= B; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Ep[s][c] = Hp[s][c] = Pair{0.0f, 0.0f};
+  uint32_t mq[B + 1];  // packed material ids (even | odd << 16) of planes p, p-1, ..., p-B
+#pragma unroll
+  for (int s = 0; s <= B; ++s) mq[s] = 0;
+
+  const int o = ly * K::W + cx0;
+  const int oym = (ly > 0 ? ly - 1 : 0) * K::W + cx0;
+  const int oyp = (ly < TY - 1 ? ly + 1 : TY - 1) * K::W + cx0;
+  const int om = ly * kMatBoxX2 + cx0 + (X - X8);  // even: a 4-byte aligned id pair
+  const float dx = a.dx;
+  const long long pitch = g.pitch, plane = g.plane;
+
+  int it = 0;
+  bool abort = false;
+  for (; it < niter; ++it) {
+    const int p = ps + it;
+    const int stage = it % K::NS;
+    if (!mbar_wait_bounded(&bars[stage], (uint32_t)(it / K::NS) & 1u, kWaitLimit)) {
+      s_abort = 1;
+      atomicExch(a.err, kErrTimeout);
+    }
+    if (B == 1) __syncthreads();  // orders last iteration's ebuf writes before this read
+    const bool mon_iter = p >= mon_lo && p <= mon_hi;
+    const bool src_iter = smask != 0 && p >= src_lo && p <= src_hi;
+
+    const float* S0 = st_f + stage * 6 * K::PL;
+#pragma unroll
+    for (int s = B; s >= 1; --s) mq[s] = mq[s - 1];
+    mq[0] = *reinterpret_cast<const uint32_t*>(st_m + stage * K::MPL + om);
+    Pair Hc[3], Eo[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float2 hv = ld2(S0 + (3 + c) * K::PL + o);
+      const float2 ev = ld2(S0 + c * K::PL + o);
+      Hc[c] = Pair{hv.x, hv.y};
+      Eo[c] = Pair{ev.x, ev.y};
+    }
+    float2 hz_ym = ld2(S0 + 5 * K::PL + oym), hx_ym = ld2(S0 + 3 * K::PL + oym);
+    Pair EnPrev[3] = {};
+    Pair EnB[3] = {}, HnB[3] = {};
+
+#pragma unroll
+    for (int s = 1; s <= B; ++s) {
+      const int e = p - s + 1;
+      const long long t = a.t0 + (s - 1);
+      // ---------------- E^s(e)
+      // x-1 neighbour: odd cell of lane-1 for the even cell, own even cell for the odd cell
+      const float hz_xm = __shfl_up_sync(kFull, Hc[2].b, 1);
+      const float hy_xm = __shfl_up_sync(kFull, Hc[1].b, 1);
+      Pair cxp, cyp, czp;
+      cxp.a = sub(sub(Hc[2].a, hz_ym.x), sub(Hc[1].a, Hp[s - 1][1].a));
+      cxp.b = sub(sub(Hc[2].b, hz_ym.y), sub(Hc[1].b, Hp[s - 1][1].b));
+      cyp.a = sub(sub(Hc[0].a, Hp[s - 1][0].a), sub(Hc[2].a, hz_xm));
+      cyp.b = sub(sub(Hc[0].b, Hp[s - 1][0].b), sub(Hc[2].b, Hc[2].a));
+      czp.a = sub(sub(Hc[1].a, hy_xm), sub(Hc[0].a, hx_ym.x));
+      czp.b = sub(sub(Hc[1].b, Hc[1].a), sub(Hc[0].b, hx_ym.y));
+      Pair En[3] = {Eo[0], Eo[1], Eo[2]};
+      const bool zint_e = e >= 1 && e <= g.nz - 2;
+      if (zint_e) {
+        if (src_iter) {
+          float v;
+          if (source_value(a.S, 0, x0, y, e, t, &v)) cxp.a = sub(cxp.a, mul(v, dx));
+          if (source_value(a.S, 1, x0, y, e, t, &v)) cyp.a = sub(cyp.a, mul(v, dx));
+          if (source_value(a.S, 2, x0, y, e, t, &v)) czp.a = sub(czp.a, mul(v, dx));
+          if (source_value(a.S, 0, x1, y, e, t, &v)) cxp.b = sub(cxp.b, mul(v, dx));
+          if (source_value(a.S, 1, x1, y, e, t, &v)) cyp.b = sub(cyp.b, mul(v, dx));
+          if (source_value(a.S, 2, x1, y, e, t, &v)) czp.b = sub(czp.b, mul(v, dx));
+        }
+        const Material* m0 = a.table + (mq[s - 1] & 0xFFFFu);
+        const Material* m1 = a.table + (mq[s - 1] >> 16);
+        const float4 a0 = __ldg(&m0->a), b0 = __ldg(&m0->b);
+        const float4 a1 = __ldg(&m1->a), b1 = __ldg(&m1->b);
+        if (int0) {
+          En[0].a = yee(a0.x, Eo[0].a, a0.y, cxp.a);
+          En[1].a = yee(a0.z, Eo[1].a, a0.w, cyp.a);
+          En[2].a = yee(b0.x, Eo[2].a, b0.y, czp.a);
+        }
+        if (int1) {
+          En[0].b = yee(a1.x, Eo[0].b, a1.y, cxp.b);
+          En[1].b = yee(a1.z, Eo[1].b, a1.w, cyp.b);
+          En[2].b = yee(b1.x, Eo[2].b, b1.y, czp.b);
+        }
+      }
+      // ---------------- H^s(e-1)
+      // x+1 neighbour: own odd cell for the even cell, even cell of lane+1 for the odd cell
+      const float ez_xp = __shfl_down_sync(kFull, Ep[s][2].a, 1);
+      const float ey_xp = __shfl_down_sync(kFull, Ep[s][1].a, 1);
+      float* eb = ebuf + (s - 1) * 2 * K::PL;
+      const float2 ex_yp = ld2(eb + oyp), ez_yp = ld2(eb + K::PL + oyp);
+      cxp.a = sub(sub(En[1].a, Ep[s][1].a), sub(ez_yp.x, Ep[s][2].a));
+      cxp.b = sub(sub(En[1].b, Ep[s][1].b), sub(ez_yp.y, Ep[s][2].b));
+      cyp.a = sub(sub(Ep[s][2].b, Ep[s][2].a), sub(En[0].a, Ep[s][0].a));
+      cyp.b = sub(sub(ez_xp, Ep[s][2].b), sub(En[0].b, Ep[s][0].b));
+      czp.a = sub(sub(ex_yp.x, Ep[s][0].a), sub(Ep[s][1].b, Ep[s][1].a));
+      czp.b = sub(sub(ex_yp.y, Ep[s][0].b), sub(ey_xp, Ep[s][1].b));
+      Pair Hn[3] = {Hp[s - 1][0], Hp[s - 1][1], Hp[s - 1][2]};
+      const bool zint_h = e - 1 >= 1 && e - 1 <= g.nz - 2;
+      if (zint_h) {
+        if (src_iter) {
+          float v;
+          if (source_value(a.S, 3, x0, y, e - 1, t, &v)) cxp.a = sub(cxp.a, mul(v, dx));
+          if (source_value(a.S, 4, x0, y, e - 1, t, &v)) cyp.a = sub(cyp.a, mul(v, dx));
+          if (source_value(a.S, 5, x0, y, e - 1, t, &v)) czp.a = sub(czp.a, mul(v, dx));
+          if (source_value(a.S, 3, x1, y, e - 1, t, &v)) cxp.b = sub(cxp.b, mul(v, dx));
+          if (source_value(a.S, 4, x1, y, e - 1, t, &v)) cyp.b = sub(cyp.b, mul(v, dx));
+          if (source_value(a.S, 5, x1, y, e - 1, t, &v)) czp.b = sub(czp.b, mul(v, dx));
+        }
+        const Material* m0 = a.table + (mq[s] & 0xFFFFu);
+        const Material* m1 = a.table + (mq[s] >> 16);
+        const float4 b0 = __ldg(&m0->b), c0 = __ldg(&m0->c);
+        const float4 b1 = __ldg(&m1->b), c1 = __ldg(&m1->c);
+        if (int0) {
+          Hn[0].a = yee(b0.z, Hp[s - 1][0].a, b0.w, cxp.a);
+          Hn[1].a = yee(c0.x, Hp[s - 1][1].a, c0.y, cyp.a);
+          Hn[2].a = yee(c0.z, Hp[s - 1][2].a, c0.w, czp.a);
+        }
+        if (int1) {
+          Hn[0].b = yee(b1.z, Hp[s - 1][0].b, b1.w, cxp.b);
+          Hn[1].b = yee(c1.x, Hp[s - 1][1].b, c1.y, cyp.b);
+          Hn[2].b = yee(c1.z, Hp[s - 1][2].b, c1.w, czp.b);
+        }
+      }
+      // ---------------- running DFT
+      if (mon_iter && (out0 || out1)) {
+        for (int n = 0; n < a.M.n; ++n) {
+          const MonitorDev& m = a.M.m[n];
+          const int mk = m.comp < 3 ? e : e - 1;
+          if (m.k == mk && mk >= z0 && mk < z1) {
+            const int c = m.comp < 3 ? m.comp : m.comp - 3;
+            const Pair v = m.comp < 3 ? (c == 0 ? En[0] : (c == 1 ? En[1] : En[2]))
+                                      : (c == 0 ? Hn[0] : (c == 1 ? Hn[1] : Hn[2]));
+            if (out0) dft_accumulate(m, t, x0, y, g, v.a);
+            if (out1) dft_accumulate(m, t, x1, y, g, v.b);
+          }
+        }
+      }
+      // ---------------- exchange
+      if (s < B) {
+        float* hb = hbuf + (s & 1) * 2 * K::PL;
+        st2(hb + o, Hn[2].a, Hn[2].b);
+        st2(hb + K::PL + o, Hn[0].a, Hn[0].b);
+      }
+      __syncthreads();
+      st2(eb + o, En[0].a, En[0].b);
+      st2(eb + K::PL + o, En[2].a, En[2].b);
+      if (s == 1) {
+        abort = s_abort != 0;
+        if (!abort && tid == 0 && it + K::NS < niter) {
+          fence_proxy_async_smem();
+          issue(it + K::NS);
+        }
+      }
+      // ---------------- rotate
+      if (s >= 2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Ep[s - 1][c] = EnPrev[c];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        EnPrev[c] = En[c];
+        Hp[s - 1][c] = Hc[c];
+      }
+      if (s < B) {
+        const float* hb = hbuf + (s & 1) * 2 * K::PL;
+        hz_ym = ld2(hb + oym);
+        hx_ym = ld2(hb + K::PL + oym);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          Hc[c] = Hn[c];
+          Eo[c] = Ep[s][c];
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          EnB[c] = En[c];
+          HnB[c] = Hn[c];
+        }
+      }
+      if (abort) break;
+    }
+    if (abort) break;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Ep[B][c] = EnPrev[c];
+
+    // ---------------- level-BLT results: E at plane p-B+1, H at plane p-B
+    if (out0 || out1) {
+      const int eB = p - B + 1, hB = p - B;
+      const bool both = out0 && out1;
+      if (eB >= z0 && eB < z1) {
+        const long long idx = x0 + (long long)y * pitch + (long long)eB * plane;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (both) st2(a.dst.f[c] + idx, EnB[c].a, EnB[c].b);
+          else if (out0) a.dst.f[c][idx] = EnB[c].a;
+          else a.dst.f[c][idx + 1] = EnB[c].b;
+        }
+      }
+      if (hB >= z0 && hB < z1) {
+        const long long idx = x0 + (long long)y * pitch + (long long)hB * plane;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (both) st2(a.dst.f[3 + c] + idx, HnB[c].a, HnB[c].b);
+          else if (out0) a.dst.f[3 + c][idx] = HnB[c].a;
+          else a.dst.f[3 + c][idx + 1] = HnB[c].b;
+        }
+      }
+    }
+  }
+
+  if (abort && tid == 0) {
+    for (int q = it + 1; q < niter && q < it + K::NS; ++q)
+      (void)mbar_wait_bounded(&bars[q % K::NS], (uint32_t)(q / K::NS) & 1u, kWaitLimit / 8);
+  }
+}
+
+template <int B, int TY>
+cudaError_t launch_one2(const TiledArgs& a, dim3 grid, cudaStream_t st) {
+  using K = Tiled2<B, TY>;
+  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2<B, TY>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
+  if (e != cudaSuccess) return e;
+  fdtd_tiled2<B, TY><<<grid, dim3(32, TY), K::SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int TY>
+cudaError_t launch_rows2(int blt, const TiledArgs& a, dim3 grid, cudaStream_t st) {
+  switch (blt) {
+    case 1: return launch_one2<1, TY>(a, grid, st);
+    case 2: return launch_one2<2, TY>(a, grid, st);
+    case 3: if constexpr (TY < 32) return launch_one2<3, TY>(a, grid, st); break;
+    case 4: if constexpr (TY == 16) return launch_one2<4, TY>(a, grid, st); break;
+    default: break;
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+bool tiled2_config_supported(const TiledConfig& c) {
+  if (c.rows != 8 && c.rows != 16 && c.rows != 32) return false;
+  if (c.blt < 1 || c.blt > 4) return false;
+  if (c.rows == 8 && c.blt > 3) return false;
+  if (c.rows == 32 && c.blt > 2) return false;  // 1024 threads: the pair state spills
+  return c.z_chunks >= 1;
+}
+
+dim3 tiled2_grid(const TiledConfig& c, const Grid& g) {
+  const int sx = tiled2_sx(c.blt), sy = tiled_sy(c.blt, c.rows);
+  const int first = tiled_xbase(c.blt) + c.blt;
+  const int ntx = (g.nx - first + sx - 1) / sx;
+  const int nty = (g.ny + sy - 1) / sy;
+  const int zlen = (g.nz + c.z_chunks - 1) / c.z_chunks;
+  const int nzc = (g.nz + zlen - 1) / zlen;
+  return dim3(ntx, nty, nzc);
+}
+
+cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& a, const Grid& g,
+                          cudaStream_t st) {
+  if (!tiled2_config_supported(c)) return cudaErrorInvalidValue;
+  const dim3 grid = tiled2_grid(c, g);
+  switch (c.rows) {
+    case 8: return launch_rows2<8>(c.blt, a, grid, st);
+    case 16: return launch_rows2<16>(c.blt, a, grid, st);
+    case 32: return launch_rows2<32>(c.blt, a, grid, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace fdtd

@@ -61,8 +61,11 @@ typedef enum fdtd_source_kind {
  * else NAIVE. */
 typedef enum fdtd_kernel {
   FDTD_KERNEL_AUTO = 0,
-  FDTD_KERNEL_NAIVE = 1,  /* one thread per cell, separate E and H launches per step */
-  FDTD_KERNEL_TILED = 2   /* z-streaming temporally tiled kernel, BLT steps per launch */
+  FDTD_KERNEL_NAIVE = 1,      /* one thread per cell, separate E and H launches per step */
+  FDTD_KERNEL_TILED = 2,      /* z-streaming temporally tiled kernel, BLT steps per launch;
+                                 the autotuner picks the family below */
+  FDTD_KERNEL_TILED_W32 = 3,  /* tiled, one cell per thread (32-wide warp rows) */
+  FDTD_KERNEL_TILED_W64 = 4   /* tiled, an x-pair of cells per thread (64-wide warp rows) */
 } fdtd_kernel;
 
 /* Field storage in HBM.  Arithmetic is FP32 in every case; F16/BF16 store each component
@@ -149,7 +152,8 @@ fdtd_status fdtd_get_field_device(fdtd_handle* h, int32_t component, float* dev_
 fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6);
 
 /* Kernel configuration actually used by the last fdtd_step: out = {kernel, blt, tile_rows,
- * z_chunks, launches in the last fdtd_step}. */
+ * z_chunks, launches in the last fdtd_step}; kernel is FDTD_KERNEL_NAIVE, _TILED_W32 or
+ * _TILED_W64. */
 fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out5);
 
 /* Builds a material map from 12 device coefficient arrays without allocating anything.

@@ -98,26 +98,30 @@ def test_vacuum_gaussian_jz_100cube():
         assert_fields_match(F, F_ref, kernel)
 
 
-CONFIGS = [(b, r, z) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)), (32, (1, 2, 4, 6)))
+CONFIGS = [(b, r, z, "tiled_w32") for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)),
+                                                (32, (1, 2, 3, 4, 5, 6)))
            for b in bs for z in (1, 3)]
+CONFIGS += [(b, r, z, "tiled_w64") for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4)), (32, (1, 2)))
+            for b in bs for z in (1, 3)]
 
 
-@pytest.mark.parametrize("blt,rows,zc", CONFIGS)
-def test_tiled_instances_pml_point_sources(blt, rows, zc):
-    shape, T = (45, 37, 29), 13
+@pytest.mark.parametrize("blt,rows,zc,family", CONFIGS)
+def test_tiled_instances_pml_point_sources(blt, rows, zc, family):
+    shape, T = (75 if family == "tiled_w64" else 45, 37, 29), 13
     coefs = W.reference_coefficients(shape)
     w = W.gaussian_wave(T, delay=4.0, width=2.0, period=5.0)
     sources = [dict(component="Jz", wave=w, i=22, j=18, k=14),
                dict(component="Mx", wave=w * np.float32(0.5), i=3, j=30, k=20),
                dict(component="Jy", wave=w, i=1, j=1, k=1)]
     F_ref = oracle.run(shape, coefs, T, sources=[osrc(s) for s in sources])
-    F, _, cfg = gpu_run(shape, coefs, T, sources, kernel="tiled", blt=blt, tile_rows=rows,
+    F, _, cfg = gpu_run(shape, coefs, T, sources, kernel=family, blt=blt, tile_rows=rows,
                         z_chunks=zc)
     assert (cfg["blt"], cfg["tile_rows"], cfg["z_chunks"]) == (blt, rows, zc)
-    assert_fields_match(F, F_ref, f"blt={blt} rows={rows} zc={zc}")
+    assert cfg["width"] == (64 if family == "tiled_w64" else 32)
+    assert_fields_match(F, F_ref, f"{family} blt={blt} rows={rows} zc={zc}")
 
 
-@pytest.mark.parametrize("kernel", ["naive", "tiled"])
+@pytest.mark.parametrize("kernel", ["naive", "tiled_w32", "tiled_w64"])
 def test_plane_source_random_eps_and_monitors(kernel):
     shape, T = (64, 48, 40), 60
     nx, ny, nz = shape

@@ -25,26 +25,29 @@ def bits_equal(a, b):
                           np.asarray(b, np.float32).view(np.uint32))
 
 
-CONFIGS = [(b, r, z) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)), (32, (1, 4, 6)))
+CONFIGS = [(b, r, z, 32) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)), (32, (1, 4, 6)))
            for b in bs for z in (1, 3)]
+CONFIGS += [(b, r, z, 64) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4)), (32, (1, 2)))
+            for b in bs for z in (1, 3)]
 
 
-@pytest.mark.parametrize("blt,rows,zc", CONFIGS)
-def test_schedule_point_sources(blt, rows, zc):
-    shape, T = (37, 21, 19), 7
+@pytest.mark.parametrize("blt,rows,zc,width", CONFIGS)
+def test_schedule_point_sources(blt, rows, zc, width):
+    shape, T = (71 if width == 64 else 37, 21, 19), 7
     coefs = oracle.coefficients(shape)
     w = wave(T)
     F_ref = oracle.run(shape, coefs, T, sources=[
         oracle.Source("Jz", w, i=18, j=10, k=9), oracle.Source("Mx", w * np.float32(0.5), i=5, j=6, k=7)])
     F = TE.run(shape, coefs, T, blt, rows, zc, DX, sources=[
         dict(comp=2, kind=0, i=18, j=10, k=9, wave=w),
-        dict(comp=3, kind=0, i=5, j=6, k=7, wave=w * np.float32(0.5))])
+        dict(comp=3, kind=0, i=5, j=6, k=7, wave=w * np.float32(0.5))], width=width)
     for c in range(6):
         assert bits_equal(F[c], F_ref[c]), oracle.COMPONENTS[c]
 
 
-@pytest.mark.parametrize("blt,rows,zc", [(2, 8, 2), (4, 16, 3), (3, 16, 1), (6, 32, 2)])
-def test_schedule_plane_source_and_monitors(blt, rows, zc):
+@pytest.mark.parametrize("blt,rows,zc,width", [(2, 8, 2, 32), (4, 16, 3, 32), (3, 16, 1, 32),
+                                               (6, 32, 2, 32), (3, 16, 2, 64), (2, 32, 1, 64)])
+def test_schedule_plane_source_and_monitors(blt, rows, zc, width):
     shape, T = (29, 23, 17), 9
     nx, ny, nz = shape
     rng = np.random.default_rng(1)
@@ -62,7 +65,8 @@ def test_schedule_plane_source_and_monitors(blt, rows, zc):
              dict(comp=4, k=5, cos=ct, sin=st, scale=1.0, re=np.zeros((3, ny, nx)),
                   im=np.zeros((3, ny, nx)))]
     F = TE.run(shape, coefs, T, blt, rows, zc, DX,
-               sources=[dict(comp=2, kind=1, i=0, j=0, k=4, wave=w)], monitors=emons)
+               sources=[dict(comp=2, kind=1, i=0, j=0, k=4, wave=w)], monitors=emons,
+               width=width)
     for c in range(6):
         assert bits_equal(F[c], F_ref[c]), oracle.COMPONENTS[c]
     for em, om in zip(emons, mons):
@@ -72,20 +76,20 @@ def test_schedule_plane_source_and_monitors(blt, rows, zc):
 
 def test_output_windows_tile_the_grid():
     """Every cell is written exactly once per pass and nothing outside the grid."""
-    for blt in range(1, 7):
-        for rows in (8, 16, 32):
-            if rows - 2 * blt < 1:
-                continue
-            for shape in ((3, 3, 3), (33, 17, 9), (100, 61, 5)):
-                nx, ny, nz = shape
-                sx, xbase, sy = TE.tile_geometry(blt, rows)
-                assert sx % 4 == 0 and xbase % 4 == 0 and xbase + blt <= 0
-                ntx, nty, nzc, zlen = TE.grid_dims(shape, blt, rows, 2)
-                cover = np.zeros(nx, int)
-                for bx in range(ntx):
-                    lo = bx * sx + xbase + blt
-                    for x in range(lo, lo + sx):
-                        if 0 <= x < nx:
-                            cover[x] += 1
-                assert (cover == 1).all()
-                assert xbase + blt + ntx * sx >= nx and nty * sy >= ny and nzc * zlen >= nz
+    for width, blt, rows in [(w, b, r) for w in (32, 64) for b in range(1, 7) for r in (8, 16, 32)]:
+        if rows - 2 * blt < 1:
+            continue
+        for shape in ((3, 3, 3), (33, 17, 9), (100, 61, 5)):
+            nx, ny, nz = shape
+            sx, xbase, sy = TE.tile_geometry(blt, rows, width)
+            assert sx % 4 == 0 and xbase % 4 == 0 and xbase + blt <= 0
+            assert sx <= width - 2 * blt
+            ntx, nty, nzc, zlen = TE.grid_dims(shape, blt, rows, 2, width)
+            cover = np.zeros(nx, int)
+            for bx in range(ntx):
+                lo = bx * sx + xbase + blt
+                for x in range(lo, lo + sx):
+                    if 0 <= x < nx:
+                        cover[x] += 1
+            assert (cover == 1).all()
+            assert xbase + blt + ntx * sx >= nx and nty * sy >= ny and nzc * zlen >= nz

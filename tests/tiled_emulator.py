@@ -16,16 +16,16 @@ from __future__ import annotations
 import numpy as np
 
 
-def tile_geometry(blt, rows):
-    sx = 4 * ((32 - 2 * blt) // 4)
+def tile_geometry(blt, rows, width=32):
+    sx = 4 * ((width - 2 * blt) // 4)
     xbase = -4 * ((blt + 3) // 4)
     sy = rows - 2 * blt
     return sx, xbase, sy
 
 
-def grid_dims(shape, blt, rows, z_chunks):
+def grid_dims(shape, blt, rows, z_chunks, width=32):
     nx, ny, nz = shape
-    sx, xbase, sy = tile_geometry(blt, rows)
+    sx, xbase, sy = tile_geometry(blt, rows, width)
     first = xbase + blt
     ntx = -(-(nx - first) // sx)
     nty = -(-ny // sy)
@@ -55,15 +55,22 @@ def _plane(F3, X, Y, z, width, rows):
     return out
 
 
-def _shfl_up(v):
+def _shfl_up(v, width):
+    """x-1 neighbour.  Width 32 (one cell per lane): lane 0 gets its own value.  Width 64 (an
+    x-pair per lane): cell 0 gets cell 1, the odd cell of its own lane."""
     out = v.copy()
     out[:, 1:] = v[:, :-1]
+    if width == 64:
+        out[:, 0] = v[:, 1]
     return out
 
 
-def _shfl_down(v):
+def _shfl_down(v, width):
+    """x+1 neighbour; at the upper edge lane 31 gets its own value (width 64: cell 62)."""
     out = v.copy()
     out[:, :-1] = v[:, 1:]
+    if width == 64:
+        out[:, -1] = v[:, -2]
     return out
 
 
@@ -84,17 +91,19 @@ def _source_value(sources, comp, x, y, e, t, dx):
     return acc, any_
 
 
-def tiled_pass(shape, F, mat, table, blt, rows, z_chunks, t0, dx, sources=(), monitors=()):
-    """One launch: BLT steps from field set F (6 flat float32 arrays) into a new set."""
+def tiled_pass(shape, F, mat, table, blt, rows, z_chunks, t0, dx, sources=(), monitors=(),
+               width=32):
+    """One launch: BLT steps from field set F (6 flat float32 arrays) into a new set.
+    width 32 emulates fdtd_tiled (k_tiled.cu), width 64 fdtd_tiled2 (k_tiled2.cu)."""
     nx, ny, nz = shape
-    B, TY = blt, rows
-    sx, xbase, sy = tile_geometry(B, TY)
-    ntx, nty, nzc, zlen = grid_dims(shape, B, TY, z_chunks)
+    B, TY, W = blt, rows, width
+    sx, xbase, sy = tile_geometry(B, TY, W)
+    ntx, nty, nzc, zlen = grid_dims(shape, B, TY, z_chunks, W)
     F3 = [np.asarray(f, np.float32).reshape(nz, ny, nx) for f in F]
     M3 = mat.reshape(nz, ny, nx)
     dst = [np.full((nz, ny, nx), np.nan, np.float32) for _ in range(6)]
     dx = np.float32(dx)
-    lx = np.arange(32)[None, :]
+    lx = np.arange(W)[None, :]
     ly = np.arange(TY)[:, None]
     f32 = np.float32
     for bz in range(nzc):
@@ -113,18 +122,18 @@ def tiled_pass(shape, F, mat, table, blt, rows, z_chunks, t0, dx, sources=(), mo
                 col_int = (x >= 1) & (x <= nx - 2) & (y >= 1) & (y <= ny - 2)
                 col_out = ((lx >= B) & (lx < B + sx) & (ly >= B) & (ly < TY - B) & (x >= 0)
                            & (x < nx) & (y >= 0) & (y < ny))
-                Ep = np.zeros((B + 1, 3, TY, 32), f32)
-                Hp = np.zeros((B + 1, 3, TY, 32), f32)
-                mq = np.zeros((B + 1, TY, 32), np.int64)
-                hbuf = np.zeros((2, 2, TY, 32), f32)
-                ebuf = np.zeros((B, 2, TY, 32), f32)
+                Ep = np.zeros((B + 1, 3, TY, W), f32)
+                Hp = np.zeros((B + 1, 3, TY, W), f32)
+                mq = np.zeros((B + 1, TY, W), np.int64)
+                hbuf = np.zeros((2, 2, TY, W), f32)
+                ebuf = np.zeros((B, 2, TY, W), f32)
                 ym = np.maximum(np.arange(TY) - 1, 0)
                 yp = np.minimum(np.arange(TY) + 1, TY - 1)
                 for it in range(niter):
                     p = ps + it
-                    S = [_plane(F3[c], X, Y, p, 32, TY) for c in range(6)]
+                    S = [_plane(F3[c], X, Y, p, W, TY) for c in range(6)]
                     mq[1:] = mq[:-1].copy()
-                    mq[0] = _plane(M3, X, Y, p, 32, TY)
+                    mq[0] = _plane(M3, X, Y, p, W, TY)
                     Hc = [S[3], S[4], S[5]]
                     hz_ym, hx_ym = S[5][ym], S[3][ym]
                     Eo = [S[0], S[1], S[2]]
@@ -132,7 +141,7 @@ def tiled_pass(shape, F, mat, table, blt, rows, z_chunks, t0, dx, sources=(), mo
                     for s in range(1, B + 1):
                         e = p - s + 1
                         t = t0 + s - 1
-                        hz_xm, hy_xm = _shfl_up(Hc[2]), _shfl_up(Hc[1])
+                        hz_xm, hy_xm = _shfl_up(Hc[2], W), _shfl_up(Hc[1], W)
                         cx = (Hc[2] - hz_ym) - (Hc[1] - Hp[s - 1][1])
                         cy = (Hc[0] - Hp[s - 1][0]) - (Hc[2] - hz_xm)
                         cz = (Hc[1] - hy_xm) - (Hc[0] - hx_ym)
@@ -146,7 +155,7 @@ def tiled_pass(shape, F, mat, table, blt, rows, z_chunks, t0, dx, sources=(), mo
                             for c in range(3):
                                 new = tb[..., c] * Eo[c] + tb[..., 3 + c] * cs[c]
                                 En[c] = np.where(col_int, new, Eo[c]).astype(f32)
-                        ez_xp, ey_xp = _shfl_down(Ep[s][2]), _shfl_down(Ep[s][1])
+                        ez_xp, ey_xp = _shfl_down(Ep[s][2], W), _shfl_down(Ep[s][1], W)
                         ex_yp, ez_yp = ebuf[s - 1][0][yp], ebuf[s - 1][1][yp]
                         cx = (En[1] - Ep[s][1]) - (ez_yp - Ep[s][2])
                         cy = (ez_xp - Ep[s][2]) - (En[0] - Ep[s][0])
@@ -200,7 +209,8 @@ def tiled_pass(shape, F, mat, table, blt, rows, z_chunks, t0, dx, sources=(), mo
     return [d.reshape(-1) for d in dst]
 
 
-def run(shape, coefs, T, blt, rows, z_chunks, dx, sources=(), monitors=(), fields=None):
+def run(shape, coefs, T, blt, rows, z_chunks, dx, sources=(), monitors=(), fields=None,
+        width=32):
     """T steps in passes of BLT (a final shorter pass for the remainder), as fdtd_step."""
     nx, ny, nz = shape
     mat, table = material_table(coefs)
@@ -208,6 +218,6 @@ def run(shape, coefs, T, blt, rows, z_chunks, dx, sources=(), monitors=(), field
     t = 0
     while t < T:
         b = min(blt, T - t)
-        F = tiled_pass(shape, F, mat, table, b, rows, z_chunks, t, dx, sources, monitors)
+        F = tiled_pass(shape, F, mat, table, b, rows, z_chunks, t, dx, sources, monitors, width)
         t += b
     return F
