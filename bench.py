@@ -222,7 +222,7 @@ def run_ours(args):
     src = [dict(component="Jz", wave=wave, i=nx // 2, j=ny // 2, k=nz // 2)]
 
     sim = gd.Simulation(nx, ny, nz, device=local, kernel=args.kernel, blt=args.blt,
-                        tile_rows=args.rows, z_chunks=args.zchunks)
+                        tile_rows=args.rows, z_chunks=args.zchunks, min_blocks=args.min_blocks)
     sim.set_coefficients(coefs)
     sim.set_sources(src)
     mid = sim.add_dft_monitor("Ez", nz // 2, freqs, scale=1.0)
@@ -329,6 +329,7 @@ def run_ours(args):
                    "dft_freqs": N_FREQS, "kernel": cfg["kernel"], "width": cfg.get("width"),
                    "blt": cfg["blt"],
                    "tile_rows": cfg["tile_rows"], "z_chunks": cfg["z_chunks"],
+                   "min_blocks": cfg["min_blocks"],
                    "parallelism": f"replicas{world}",
                    "l2": "inputs (1.2 GB of fields) larger than L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -360,6 +361,7 @@ def main():
     ap.add_argument("--blt", type=int, default=0, help="force time steps per launch")
     ap.add_argument("--rows", type=int, default=0, help="force tile rows")
     ap.add_argument("--zchunks", type=int, default=0, help="force z-chunks")
+    ap.add_argument("--min-blocks", type=int, default=0, help="force the register cap")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

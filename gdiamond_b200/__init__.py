@@ -46,7 +46,8 @@ class FdtdError(RuntimeError):
 class _Desc(C.Structure):
     _fields_ = [("nx", C.c_int64), ("ny", C.c_int64), ("nz", C.c_int64), ("dx", C.c_float),
                 ("device", C.c_int32), ("storage", C.c_int32), ("kernel", C.c_int32),
-                ("blt", C.c_int32), ("tile_rows", C.c_int32), ("z_chunks", C.c_int32)]
+                ("blt", C.c_int32), ("tile_rows", C.c_int32), ("z_chunks", C.c_int32),
+                ("min_blocks", C.c_int32)]
 
 
 class _Source(C.Structure):
@@ -109,11 +110,11 @@ class Simulation:
     """
 
     def __init__(self, nx, ny, nz, dx=np.float32(0.1), device=0, kernel="auto", blt=0,
-                 tile_rows=0, z_chunks=0, storage="f32"):
+                 tile_rows=0, z_chunks=0, storage="f32", min_blocks=0):
         self.shape = (int(nx), int(ny), int(nz))
         self._L = library()
         d = _Desc(nx, ny, nz, float(np.float32(dx)), device, STORAGE[storage], KERNELS[kernel],
-                  blt, tile_rows, z_chunks)
+                  blt, tile_rows, z_chunks, min_blocks)
         h = C.c_void_p()
         st = self._L.fdtd_create(C.byref(d), C.byref(h))
         if st != 0:
@@ -218,12 +219,12 @@ class Simulation:
         return v.value
 
     def config(self):
-        out = (C.c_int32 * 5)()
+        out = (C.c_int32 * 6)()
         self._check(self._L.fdtd_get_config(self._h, out))
         kernel = {1: "naive", 3: "tiled", 4: "tiled"}.get(out[0], "none")
         width = {3: 32, 4: 64}.get(out[0], 0)
         return {"kernel": kernel, "width": width, "blt": out[1], "tile_rows": out[2],
-                "z_chunks": out[3], "launches": out[4]}
+                "z_chunks": out[3], "launches": out[4], "min_blocks": out[5]}
 
     # ---------------------------------------------------------------- results
     def get_field(self, component, out=None):

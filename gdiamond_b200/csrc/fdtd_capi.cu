@@ -264,13 +264,15 @@ std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
   for (int w : widths)
     for (int rows : rows_l)
       for (int b : blts)
-        for (int z : zc) {
-          fdtd::TiledConfig c{b, rows, z, w};
-          if (!config_supported(c)) continue;
-          // A chunk shorter than its 2*BLT warm-up is only worth it when asked for.
-          if (!forced_z && (h->g.nz + z - 1) / z < 2 * b) continue;
-          out.push_back(c);
-        }
+        for (int z : zc)
+          for (int mb : {1, 2, 4}) {
+            if (h->desc.min_blocks > 0 && mb != h->desc.min_blocks) continue;
+            fdtd::TiledConfig c{b, rows, z, w, mb};
+            if (!config_supported(c)) continue;
+            // A chunk shorter than its 2*BLT warm-up is only worth it when asked for.
+            if (!forced_z && (h->g.nz + z - 1) / z < 2 * b) continue;
+            out.push_back(c);
+          }
   return out;
 }
 
@@ -278,8 +280,9 @@ std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
 // and monitors off, so the simulation state is not changed) and keeps the fastest per step.
 fdtd_status autotune(fdtd_handle* h, cudaStream_t st) {
   const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz,
-                                   h->desc.kernel * 1000000 + h->desc.blt * 10000 +
-                                       h->desc.tile_rows * 100 + h->desc.z_chunks);
+                                   h->desc.min_blocks * 100000000 + h->desc.kernel * 1000000 +
+                                       h->desc.blt * 10000 + h->desc.tile_rows * 100 +
+                                       h->desc.z_chunks);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -452,6 +455,8 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
   if (d->tile_rows != 0 && d->tile_rows != 8 && d->tile_rows != 16 && d->tile_rows != 32)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "tile_rows must be 0, 8, 16 or 32");
   if (d->z_chunks < 0) return fail(nullptr, FDTD_ERR_INVALID_ARG, "z_chunks must be >= 0");
+  if (d->min_blocks != 0 && d->min_blocks != 1 && d->min_blocks != 2 && d->min_blocks != 4)
+    return fail(nullptr, FDTD_ERR_INVALID_ARG, "min_blocks must be 0, 1, 2 or 4");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(nullptr, FDTD_ERR_CUDA, "no CUDA device available");
@@ -651,7 +656,10 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
     int64_t left = T;
     while (left > 0) {
       fdtd::TiledConfig cc = c;
-      if (left < c.blt) cc.blt = (int)left;
+      if (left < c.blt) {  // a shorter final pass (plain register allocation)
+        cc.blt = (int)left;
+        cc.min_blocks = 1;
+      }
       const fdtd::TiledArgs a = make_tiled_args(h, cc, h->t, true);
       CUDA_TRY(h, launch_any(cc, a, h->g, st));
       ++launches;
@@ -733,13 +741,14 @@ fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6) {
   return fail(h, FDTD_ERR_UNSUPPORTED, "reduced-precision storage is not built");
 }
 
-fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out5) {
-  if (!h || !out5) return FDTD_ERR_INVALID_ARG;
-  out5[0] = h->last_kernel;
-  out5[1] = h->cfg.blt;
-  out5[2] = h->cfg.rows;
-  out5[3] = h->cfg.z_chunks;
-  out5[4] = h->last_launches;
+fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out6) {
+  if (!h || !out6) return FDTD_ERR_INVALID_ARG;
+  out6[0] = h->last_kernel;
+  out6[1] = h->cfg.blt;
+  out6[2] = h->cfg.rows;
+  out6[3] = h->cfg.z_chunks;
+  out6[4] = h->last_launches;
+  out6[5] = h->cfg.min_blocks;
   return FDTD_OK;
 }
 

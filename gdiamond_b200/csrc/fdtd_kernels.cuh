@@ -36,6 +36,7 @@ struct TiledConfig {
   int rows;       // tile rows (warps per CTA)
   int z_chunks;   // z-chunks per tile column
   int width = 32; // cells per warp row: 32 (k_tiled.cu) or 64 (k_tiled2.cu, x-pairs)
+  int min_blocks = 1;  // register cap: CTAs per SM the compiler must fit (x-pair family)
 };
 
 // Tile geometry shared by the host (grid size, tensor-map boxes) and the kernel.

@@ -48,8 +48,10 @@ __device__ __forceinline__ void st2(float* p, float a, float b) {
   *reinterpret_cast<float2*>(p) = make_float2(a, b);
 }
 
-template <int B, int TY>
-__global__ void __launch_bounds__(32 * TY) fdtd_tiled2(const __grid_constant__ TiledArgs a) {
+// MINB > 1 caps registers so that MINB CTAs fit on an SM (more warps to hide latency, at the
+// cost of some spilled state); the autotuner decides per grid whether that pays.
+template <int B, int TY, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_constant__ TiledArgs a) {
   using K = Tiled2<B, TY>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
@@ -344,23 +346,34 @@ __global__ void __launch_bounds__(32 * TY) fdtd_tiled2(const __grid_constant__ T
   }
 }
 
-template <int B, int TY>
+template <int B, int TY, int MINB>
 cudaError_t launch_one2(const TiledArgs& a, dim3 grid, cudaStream_t st) {
   using K = Tiled2<B, TY>;
-  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2<B, TY>,
+  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2<B, TY, MINB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
   if (e != cudaSuccess) return e;
-  fdtd_tiled2<B, TY><<<grid, dim3(32, TY), K::SMEM, st>>>(a);
+  fdtd_tiled2<B, TY, MINB><<<grid, dim3(32, TY), K::SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
 template <int TY>
-cudaError_t launch_rows2(int blt, const TiledArgs& a, dim3 grid, cudaStream_t st) {
+cudaError_t launch_rows2(int blt, int min_blocks, const TiledArgs& a, dim3 grid,
+                         cudaStream_t st) {
+  if (min_blocks > 1) {
+    // register-capped variants: two CTAs of 16 rows or four of 8 rows per SM
+    if constexpr (TY == 16) {
+      if (blt == 2 && min_blocks == 2) return launch_one2<2, 16, 2>(a, grid, st);
+    }
+    if constexpr (TY == 8) {
+      if (blt == 2 && min_blocks == 4) return launch_one2<2, 8, 4>(a, grid, st);
+    }
+    return cudaErrorInvalidValue;
+  }
   switch (blt) {
-    case 1: return launch_one2<1, TY>(a, grid, st);
-    case 2: return launch_one2<2, TY>(a, grid, st);
-    case 3: if constexpr (TY < 32) return launch_one2<3, TY>(a, grid, st); break;
-    case 4: if constexpr (TY == 16) return launch_one2<4, TY>(a, grid, st); break;
+    case 1: return launch_one2<1, TY, 1>(a, grid, st);
+    case 2: return launch_one2<2, TY, 1>(a, grid, st);
+    case 3: if constexpr (TY < 32) return launch_one2<3, TY, 1>(a, grid, st); break;
+    case 4: if constexpr (TY == 16) return launch_one2<4, TY, 1>(a, grid, st); break;
     default: break;
   }
   return cudaErrorInvalidValue;
@@ -373,6 +386,9 @@ bool tiled2_config_supported(const TiledConfig& c) {
   if (c.blt < 1 || c.blt > 4) return false;
   if (c.rows == 8 && c.blt > 3) return false;
   if (c.rows == 32 && c.blt > 2) return false;  // 1024 threads: the pair state spills
+  if (c.min_blocks > 1 && !(c.blt == 2 && ((c.rows == 16 && c.min_blocks == 2) ||
+                                           (c.rows == 8 && c.min_blocks == 4))))
+    return false;
   return c.z_chunks >= 1;
 }
 
@@ -391,9 +407,9 @@ cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& a, const Grid& 
   if (!tiled2_config_supported(c)) return cudaErrorInvalidValue;
   const dim3 grid = tiled2_grid(c, g);
   switch (c.rows) {
-    case 8: return launch_rows2<8>(c.blt, a, grid, st);
-    case 16: return launch_rows2<16>(c.blt, a, grid, st);
-    case 32: return launch_rows2<32>(c.blt, a, grid, st);
+    case 8: return launch_rows2<8>(c.blt, c.min_blocks, a, grid, st);
+    case 16: return launch_rows2<16>(c.blt, c.min_blocks, a, grid, st);
+    case 32: return launch_rows2<32>(c.blt, c.min_blocks, a, grid, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -85,6 +85,8 @@ typedef struct fdtd_desc {
   int32_t blt;          /* time steps per tiled launch; 0 = autotuned */
   int32_t tile_rows;    /* tiled-kernel rows per tile (8, 16 or 32); 0 = autotuned */
   int32_t z_chunks;     /* tiled-kernel z-chunks per column; 0 = autotuned */
+  int32_t min_blocks;   /* tiled x-pair family: CTAs per SM the registers must allow (1, 2 or
+                           4); 0 = autotuned */
 } fdtd_desc;
 
 typedef struct fdtd_source {
@@ -152,9 +154,9 @@ fdtd_status fdtd_get_field_device(fdtd_handle* h, int32_t component, float* dev_
 fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6);
 
 /* Kernel configuration actually used by the last fdtd_step: out = {kernel, blt, tile_rows,
- * z_chunks, launches in the last fdtd_step}; kernel is FDTD_KERNEL_NAIVE, _TILED_W32 or
- * _TILED_W64. */
-fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out5);
+ * z_chunks, launches in the last fdtd_step, min_blocks}; kernel is FDTD_KERNEL_NAIVE,
+ * _TILED_W32 or _TILED_W64. */
+fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out6);
 
 /* Builds a material map from 12 device coefficient arrays without allocating anything.
  * No counterpart in the reference (which keeps 12 per-cell arrays); it is the allocation-free

@@ -103,10 +103,15 @@ CONFIGS = [(b, r, z, "tiled_w32") for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4
            for b in bs for z in (1, 3)]
 CONFIGS += [(b, r, z, "tiled_w64") for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4)), (32, (1, 2)))
             for b in bs for z in (1, 3)]
+# register-capped x-pair variants (2 CTAs of 16 rows / 4 CTAs of 8 rows per SM)
+CONFIGS += [(2, 16, 1, "tiled_w64:2"), (2, 16, 3, "tiled_w64:2"), (2, 8, 1, "tiled_w64:4"),
+            (2, 8, 3, "tiled_w64:4")]
 
 
 @pytest.mark.parametrize("blt,rows,zc,family", CONFIGS)
 def test_tiled_instances_pml_point_sources(blt, rows, zc, family):
+    family, _, mb = family.partition(":")
+    mb = int(mb or 0)
     shape, T = (75 if family == "tiled_w64" else 45, 37, 29), 13
     coefs = W.reference_coefficients(shape)
     w = W.gaussian_wave(T, delay=4.0, width=2.0, period=5.0)
@@ -115,8 +120,9 @@ def test_tiled_instances_pml_point_sources(blt, rows, zc, family):
                dict(component="Jy", wave=w, i=1, j=1, k=1)]
     F_ref = oracle.run(shape, coefs, T, sources=[osrc(s) for s in sources])
     F, _, cfg = gpu_run(shape, coefs, T, sources, kernel=family, blt=blt, tile_rows=rows,
-                        z_chunks=zc)
+                        z_chunks=zc, min_blocks=mb)
     assert (cfg["blt"], cfg["tile_rows"], cfg["z_chunks"]) == (blt, rows, zc)
+    assert cfg["min_blocks"] == (mb or 1)
     assert cfg["width"] == (64 if family == "tiled_w64" else 32)
     assert_fields_match(F, F_ref, f"{family} blt={blt} rows={rows} zc={zc}")
 
