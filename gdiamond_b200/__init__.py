@@ -23,7 +23,7 @@ COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 SOURCE_COMPONENTS = ("Jx", "Jy", "Jz", "Mx", "My", "Mz")
 COEFFS = ("Cax", "Cay", "Caz", "Cbx", "Cby", "Cbz", "Dax", "Day", "Daz", "Dbx", "Dby", "Dbz")
 KERNELS = {"auto": 0, "naive": 1, "tiled": 2, "tiled_w32": 3, "tiled_w64": 4}
-STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
 SRC_POINT, SRC_PLANE_Z = 0, 1
 
 # Every symbol declared in include/fdtd_capi.h.
@@ -33,7 +33,9 @@ EXPORTS = (
     "fdtd_set_sources", "fdtd_add_dft_monitor", "fdtd_reset", "fdtd_step", "fdtd_sync",
     "fdtd_get_step", "fdtd_get_field", "fdtd_set_field", "fdtd_get_dft",
     "fdtd_get_field_device", "fdtd_set_storage_scale", "fdtd_get_config",
-    "fdtd_build_material_map_noalloc",
+    "fdtd_build_material_map_noalloc", "fdtd_get_field_f64",
+    "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_step", "fdtd_batch_get_config",
+    "fdtd_batch_last_error",
 )
 
 
@@ -88,6 +90,12 @@ def library():
             "fdtd_get_field_device": ([V, C.c_int32, V, V], C.c_int),
             "fdtd_set_storage_scale": ([V, P(C.c_float)], C.c_int),
             "fdtd_get_config": ([V, P(C.c_int32)], C.c_int),
+            "fdtd_get_field_f64": ([V, C.c_int32, P(C.c_double)], C.c_int),
+            "fdtd_batch_create": ([P(V), C.c_int32, P(V)], C.c_int),
+            "fdtd_batch_destroy": ([V], C.c_int),
+            "fdtd_batch_step": ([V, C.c_int64, C.c_int32, V], C.c_int),
+            "fdtd_batch_get_config": ([V, P(C.c_int32)], C.c_int),
+            "fdtd_batch_last_error": ([V], C.c_char_p),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -237,6 +245,17 @@ class Simulation:
     def fields(self):
         return [self.get_field(c) for c in range(6)]
 
+    def get_field_f64(self, component, out=None):
+        comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
+        if out is None:
+            out = np.empty(self.ncells, np.float64)
+        self._check(self._L.fdtd_get_field_f64(self._h, comp, _fp(out, C.c_double)))
+        return out
+
+    def set_storage_scale(self, scale6):
+        s = (C.c_float * 6)(*[float(v) for v in scale6])
+        self._check(self._L.fdtd_set_storage_scale(self._h, s))
+
     def set_field(self, component, values):
         comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
         v = np.ascontiguousarray(values, np.float32).reshape(-1)
@@ -259,6 +278,52 @@ class Simulation:
         self._check(self._L.fdtd_get_dft(self._h, monitor_id, _fp(re, C.c_double),
                                           _fp(im, C.c_double)))
         return re, im
+
+
+class Batch:
+    """Independent simulations advanced together by persistent launches (fdtd_batch_*).
+
+    All simulations must live on one device with one storage type and have their
+    coefficients set (compressed to a material map).  Each keeps its own fields, sources,
+    monitors and step counter; results are read from the Simulation objects as usual.
+    """
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        self._L = library()
+        arr = (C.c_void_p * len(self.sims))(*[s._h.value for s in self.sims])
+        h = C.c_void_p()
+        st = self._L.fdtd_batch_create(arr, len(self.sims), C.byref(h))
+        if st != 0:
+            raise FdtdError(st, self._L.fdtd_batch_last_error(None).decode())
+        self._h = h
+
+    def _check(self, st):
+        if st != 0:
+            raise FdtdError(st, self._L.fdtd_batch_last_error(self._h).decode())
+
+    def step(self, T, use_graph=True, stream=None):
+        s = None
+        if stream is not None:
+            s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        self._check(self._L.fdtd_batch_step(self._h, int(T), 1 if use_graph else 0, s))
+
+    def config(self):
+        out = (C.c_int32 * 6)()
+        self._check(self._L.fdtd_batch_get_config(self._h, out))
+        return {"blt": out[0], "tile_rows": out[1], "ctas": out[2], "items": out[3],
+                "launches": out[4], "graph_replayed": bool(out[5])}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fdtd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 from . import workloads  # noqa: E402,F401

@@ -93,6 +93,12 @@ struct fdtd_handle {
   CUtensorMap mat_map;
   int maps_key = 0;  // width * 1000 + rows of the encoded boxes
   int last_kernel = 0, last_launches = 0;
+  int storage = FDTD_STORE_F32;
+  int esz = 4;     // bytes per stored field value
+  int nsets = 2;   // field sets (1 for FP64: the naive kernel updates in place)
+  float scale[6] = {1, 1, 1, 1, 1, 1}, inv_scale[6] = {1, 1, 1, 1, 1, 1};
+  float* f32_stage = nullptr;   // pitched FP32 staging for field transfers of other storages
+  double* f64_stage = nullptr;  // pitched FP64 staging for fdtd_get_field_f64
   std::string err;
 };
 
@@ -156,10 +162,12 @@ fdtd_status encode_map(fdtd_handle* h, CUtensorMap* m, void* base, CUtensorMapDa
 fdtd_status ensure_maps(fdtd_handle* h, int width, int rows) {
   const int key = width * 1000 + rows;
   if (h->maps_key == key) return FDTD_OK;
+  const CUtensorMapDataType dt = h->storage == FDTD_STORE_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                 : h->storage == FDTD_STORE_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                                 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   for (int s = 0; s < 2; ++s)
     for (int c = 0; c < 6; ++c) {
-      fdtd_status st = encode_map(h, &h->maps[s][c], h->F[s][c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                                  4, width, rows);
+      fdtd_status st = encode_map(h, &h->maps[s][c], h->F[s][c], dt, h->esz, width, rows);
       if (st != FDTD_OK) return st;
     }
   const int mat_box = width == 64 ? fdtd::kMatBoxX2 : fdtd::kMatBoxX;
@@ -231,13 +239,14 @@ fdtd_status ensure_tables(fdtd_handle* h, long long upto) {
 }
 
 fdtd::TiledArgs make_tiled_args(fdtd_handle* h, const fdtd::TiledConfig& c, long long t0,
-                                bool with_io) {
+                                bool with_io, int src_set = -1) {
+  const int src = src_set < 0 ? h->cur : src_set;
   fdtd::TiledArgs a;
   memset(&a, 0, sizeof(a));
-  for (int k = 0; k < 6; ++k) a.tm_src[k] = h->maps[h->cur][k];
+  for (int k = 0; k < 6; ++k) a.tm_src[k] = h->maps[src][k];
   a.tm_mat = h->mat_map;
   a.g = h->g;
-  for (int k = 0; k < 6; ++k) a.dst.f[k] = h->F[h->cur ^ 1][k];
+  for (int k = 0; k < 6; ++k) a.dst.f[k] = h->F[src ^ 1][k];
   a.table = h->table;
   if (with_io) {
     a.S = make_sources(h);
@@ -247,6 +256,10 @@ fdtd::TiledArgs make_tiled_args(fdtd_handle* h, const fdtd::TiledConfig& c, long
   a.dx = h->desc.dx;
   a.zlen = (h->g.nz + c.z_chunks - 1) / c.z_chunks;
   a.err = h->d_err;
+  for (int k = 0; k < 6; ++k) {
+    a.scale[k] = h->scale[k];
+    a.inv_scale[k] = h->inv_scale[k];
+  }
   return a;
 }
 
@@ -255,6 +268,11 @@ std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
   std::vector<fdtd::TiledConfig> out;
   std::vector<int> blts = {1, 2, 3, 4, 5, 6}, rows_l = {8, 16, 32}, zc = {1, 2, 4, 8};
   std::vector<int> widths = {32, 64};
+  const bool half = h->esz == 2;
+  if (half) {
+    widths = {64};
+    rows_l = {8, 16};
+  }
   if (h->desc.blt > 0) blts = {h->desc.blt};
   if (h->desc.tile_rows > 0) rows_l = {h->desc.tile_rows};
   if (h->desc.z_chunks > 0) zc = {h->desc.z_chunks};
@@ -267,7 +285,7 @@ std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
         for (int z : zc)
           for (int mb : {1, 2, 4}) {
             if (h->desc.min_blocks > 0 && mb != h->desc.min_blocks) continue;
-            fdtd::TiledConfig c{b, rows, z, w, mb};
+            fdtd::TiledConfig c{b, rows, z, w, mb, h->storage, h->esz};
             if (!config_supported(c)) continue;
             // A chunk shorter than its 2*BLT warm-up is only worth it when asked for.
             if (!forced_z && (h->g.nz + z - 1) / z < 2 * b) continue;
@@ -280,9 +298,9 @@ std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
 // and monitors off, so the simulation state is not changed) and keeps the fastest per step.
 fdtd_status autotune(fdtd_handle* h, cudaStream_t st) {
   const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz,
-                                   h->desc.min_blocks * 100000000 + h->desc.kernel * 1000000 +
-                                       h->desc.blt * 10000 + h->desc.tile_rows * 100 +
-                                       h->desc.z_chunks);
+                                   h->storage * 1000000000 + h->desc.min_blocks * 100000000 +
+                                       h->desc.kernel * 1000000 + h->desc.blt * 10000 +
+                                       h->desc.tile_rows * 100 + h->desc.z_chunks);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -377,6 +395,8 @@ void free_all(fdtd_handle* h) {
   cudaFree(h->scratch);
   cudaFree(h->d_wave);
   cudaFree(h->d_err);
+  cudaFree(h->f32_stage);
+  cudaFree(h->f64_stage);
   for (int m = 0; m < h->nmon; ++m) {
     cudaFree(h->mon[m].re);
     cudaFree(h->mon[m].im);
@@ -447,10 +467,17 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "grid must be at least 3 cells per axis");
   if (d->nx > (1 << 24) || d->ny > (1 << 24) || d->nz > (1 << 24))
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "grid axis too large");
-  if (d->storage != FDTD_STORE_F32)
-    return fail(nullptr, FDTD_ERR_UNSUPPORTED, "only FP32 field storage is built");
+  if (d->storage < FDTD_STORE_F32 || d->storage > FDTD_STORE_F64)
+    return fail(nullptr, FDTD_ERR_INVALID_ARG, "unknown storage %d", d->storage);
   if (d->kernel < FDTD_KERNEL_AUTO || d->kernel > FDTD_KERNEL_TILED_W64)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "unknown kernel %d", d->kernel);
+  if ((d->storage == FDTD_STORE_F16 || d->storage == FDTD_STORE_BF16) &&
+      (d->kernel == FDTD_KERNEL_NAIVE || d->kernel == FDTD_KERNEL_TILED_W32))
+    return fail(nullptr, FDTD_ERR_UNSUPPORTED,
+                "16-bit field storage runs the tiled x-pair kernel only");
+  if (d->storage == FDTD_STORE_F64 && d->kernel != FDTD_KERNEL_AUTO &&
+      d->kernel != FDTD_KERNEL_NAIVE)
+    return fail(nullptr, FDTD_ERR_UNSUPPORTED, "FP64 field storage runs the naive kernel only");
   if (d->blt < 0 || d->blt > 6) return fail(nullptr, FDTD_ERR_INVALID_ARG, "blt must be 0..6");
   if (d->tile_rows != 0 && d->tile_rows != 8 && d->tile_rows != 16 && d->tile_rows != 32)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "tile_rows must be 0, 8, 16 or 32");
@@ -471,6 +498,9 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
   h->g.pitch = (int)((d->nx + 7) / 8 * 8);
   h->g.plane = (long long)h->g.pitch * d->ny;
   h->cells = (size_t)h->g.plane * d->nz;
+  h->storage = d->storage;
+  h->esz = d->storage == FDTD_STORE_F32 ? 4 : (d->storage == FDTD_STORE_F64 ? 8 : 2);
+  h->nsets = d->storage == FDTD_STORE_F64 ? 1 : 2;
   auto bail = [&](fdtd_status s) {
     g_create_error = h->err;
     free_all(h);
@@ -479,13 +509,13 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
   };
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(h, FDTD_ERR_CUDA, "cudaStreamCreate failed"));
-  for (int s = 0; s < 2; ++s)
+  for (int s = 0; s < h->nsets; ++s)
     for (int c = 0; c < 6; ++c) {
-      cudaError_t e = cudaMalloc(&h->F[s][c], h->cells * sizeof(float));
+      cudaError_t e = cudaMalloc(&h->F[s][c], h->cells * h->esz);
       if (e != cudaSuccess)
         return bail(fail(h, FDTD_ERR_OOM, "cudaMalloc of %zu field bytes failed: %s",
-                         h->cells * sizeof(float), cudaGetErrorString(e)));
-      cudaMemsetAsync(h->F[s][c], 0, h->cells * sizeof(float), h->stream);
+                         h->cells * (size_t)h->esz, cudaGetErrorString(e)));
+      cudaMemsetAsync(h->F[s][c], 0, h->cells * h->esz, h->stream);
     }
   if (cudaMalloc(&h->d_err, sizeof(int)) != cudaSuccess)
     return bail(fail(h, FDTD_ERR_OOM, "cudaMalloc failed"));
@@ -595,9 +625,9 @@ fdtd_status fdtd_add_dft_monitor(fdtd_handle* h, int32_t component, int64_t k,
 fdtd_status fdtd_reset(fdtd_handle* h) {
   if (!h) return FDTD_ERR_INVALID_ARG;
   DeviceGuard dg(h->desc.device);
-  for (int s = 0; s < 2; ++s)
+  for (int s = 0; s < h->nsets; ++s)
     for (int c = 0; c < 6; ++c)
-      CUDA_TRY(h, cudaMemsetAsync(h->F[s][c], 0, h->cells * sizeof(float), h->stream));
+      CUDA_TRY(h, cudaMemsetAsync(h->F[s][c], 0, h->cells * h->esz, h->stream));
   for (int m = 0; m < h->nmon; ++m) {
     const size_t bytes = (size_t)h->mon[m].nf * h->g.nx * h->g.ny * sizeof(double);
     CUDA_TRY(h, cudaMemsetAsync(h->mon[m].re, 0, bytes, h->stream));
@@ -627,7 +657,10 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
   if (s != FDTD_OK) return s;
   int kernel = h->desc.kernel;
   if (kernel == FDTD_KERNEL_AUTO)
-    kernel = h->coef_mode == kCoefMaterial ? FDTD_KERNEL_TILED : FDTD_KERNEL_NAIVE;
+    kernel = (h->coef_mode == kCoefMaterial && h->storage != FDTD_STORE_F64) ? FDTD_KERNEL_TILED
+                                                                            : FDTD_KERNEL_NAIVE;
+  if (kernel == FDTD_KERNEL_NAIVE && h->esz == 2)
+    return fail(h, FDTD_ERR_UNSUPPORTED, "16-bit field storage needs the tiled kernel");
   if (kernel != FDTD_KERNEL_NAIVE && h->coef_mode != kCoefMaterial)
     return fail(h, FDTD_ERR_UNSUPPORTED,
                 "the tiled kernel needs a material map (more than %d distinct coefficient "
@@ -641,7 +674,8 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
     const bool matm = h->coef_mode == kCoefMaterial;
     for (int64_t n = 0; n < T; ++n) {
       CUDA_TRY(h, fdtd::launch_naive_step(h->g, F, matm ? nullptr : h->coef, matm ? h->mat : nullptr,
-                                          h->table, S, M, h->t, h->desc.dx, st, &launches));
+                                          h->table, S, M, h->t, h->desc.dx, st, &launches,
+                                          h->storage == FDTD_STORE_F64));
       h->t += 1;
     }
     h->last_kernel = FDTD_KERNEL_NAIVE;
@@ -651,6 +685,8 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
       if (s != FDTD_OK) return s;
     }
     fdtd::TiledConfig c = h->cfg;
+    c.storage = h->storage;  // the kernel instance must match this handle's field storage
+    c.esz = h->esz;
     s = ensure_maps(h, c.width, c.rows);
     if (s != FDTD_OK) return s;
     int64_t left = T;
@@ -693,11 +729,41 @@ fdtd_status fdtd_get_step(const fdtd_handle* h, int64_t* t) {
   return FDTD_OK;
 }
 
+// Pitched FP32 view of a field component: the field itself for FP32 storage, else the
+// component converted into the FP32 staging buffer (asynchronous on st).
+fdtd_status f32_view(fdtd_handle* h, int32_t component, cudaStream_t st, const float** out) {
+  if (h->storage == FDTD_STORE_F32) {
+    *out = h->F[h->cur][component];
+    return FDTD_OK;
+  }
+  if (!h->f32_stage) CUDA_TRY(h, cudaMalloc(&h->f32_stage, h->cells * sizeof(float)));
+  CUDA_TRY(h, fdtd::convert_field_to_f32(h->g, h->F[h->cur][component], h->storage,
+                                         h->scale[component], h->f32_stage, st));
+  *out = h->f32_stage;
+  return FDTD_OK;
+}
+
 fdtd_status fdtd_get_field(fdtd_handle* h, int32_t component, float* host_out) {
   if (!h || !host_out || component < 0 || component > 5) return FDTD_ERR_INVALID_ARG;
   DeviceGuard dg(h->desc.device);
-  CUDA_TRY(h, cudaMemcpy2DAsync(host_out, (size_t)h->g.nx * 4, h->F[h->cur][component],
-                                (size_t)h->g.pitch * 4, (size_t)h->g.nx * 4,
+  const float* src = nullptr;
+  fdtd_status s = f32_view(h, component, h->stream, &src);
+  if (s != FDTD_OK) return s;
+  CUDA_TRY(h, cudaMemcpy2DAsync(host_out, (size_t)h->g.nx * 4, src, (size_t)h->g.pitch * 4,
+                                (size_t)h->g.nx * 4, (size_t)h->g.ny * h->g.nz,
+                                cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return check_device_error(h);
+}
+
+fdtd_status fdtd_get_field_f64(fdtd_handle* h, int32_t component, double* host_out) {
+  if (!h || !host_out || component < 0 || component > 5) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  if (!h->f64_stage) CUDA_TRY(h, cudaMalloc(&h->f64_stage, h->cells * sizeof(double)));
+  CUDA_TRY(h, fdtd::convert_field_to_f64(h->g, h->F[h->cur][component], h->storage,
+                                         h->scale[component], h->f64_stage, h->stream));
+  CUDA_TRY(h, cudaMemcpy2DAsync(host_out, (size_t)h->g.nx * 8, h->f64_stage,
+                                (size_t)h->g.pitch * 8, (size_t)h->g.nx * 8,
                                 (size_t)h->g.ny * h->g.nz, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return check_device_error(h);
@@ -707,19 +773,35 @@ fdtd_status fdtd_get_field_device(fdtd_handle* h, int32_t component, float* dev_
                                   void* stream) {
   if (!h || !dev_out || component < 0 || component > 5) return FDTD_ERR_INVALID_ARG;
   DeviceGuard dg(h->desc.device);
-  CUDA_TRY(h, cudaMemcpy2DAsync(dev_out, (size_t)h->g.nx * 4, h->F[h->cur][component],
-                                (size_t)h->g.pitch * 4, (size_t)h->g.nx * 4,
-                                (size_t)h->g.ny * h->g.nz, cudaMemcpyDeviceToDevice,
-                                pick_stream(h, stream)));
+  cudaStream_t st = pick_stream(h, stream);
+  const float* src = nullptr;
+  fdtd_status s = f32_view(h, component, st, &src);
+  if (s != FDTD_OK) return s;
+  CUDA_TRY(h, cudaMemcpy2DAsync(dev_out, (size_t)h->g.nx * 4, src, (size_t)h->g.pitch * 4,
+                                (size_t)h->g.nx * 4, (size_t)h->g.ny * h->g.nz,
+                                cudaMemcpyDeviceToDevice, st));
   return FDTD_OK;
 }
 
 fdtd_status fdtd_set_field(fdtd_handle* h, int32_t component, const float* host_in) {
   if (!h || !host_in || component < 0 || component > 5) return FDTD_ERR_INVALID_ARG;
   DeviceGuard dg(h->desc.device);
-  CUDA_TRY(h, cudaMemcpy2DAsync(h->F[h->cur][component], (size_t)h->g.pitch * 4, host_in,
-                                (size_t)h->g.nx * 4, (size_t)h->g.nx * 4,
-                                (size_t)h->g.ny * h->g.nz, cudaMemcpyHostToDevice, h->stream));
+  if (h->storage == FDTD_STORE_F32) {
+    CUDA_TRY(h, cudaMemcpy2DAsync(h->F[h->cur][component], (size_t)h->g.pitch * 4, host_in,
+                                  (size_t)h->g.nx * 4, (size_t)h->g.nx * 4,
+                                  (size_t)h->g.ny * h->g.nz, cudaMemcpyHostToDevice, h->stream));
+  } else {
+    if (!h->f32_stage) {
+      CUDA_TRY(h, cudaMalloc(&h->f32_stage, h->cells * sizeof(float)));
+      CUDA_TRY(h, cudaMemsetAsync(h->f32_stage, 0, h->cells * sizeof(float), h->stream));
+    }
+    CUDA_TRY(h, cudaMemcpy2DAsync(h->f32_stage, (size_t)h->g.pitch * 4, host_in,
+                                  (size_t)h->g.nx * 4, (size_t)h->g.nx * 4,
+                                  (size_t)h->g.ny * h->g.nz, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, fdtd::convert_field_from_f32(h->g, h->f32_stage, h->storage,
+                                             h->inv_scale[component], h->F[h->cur][component],
+                                             h->stream));
+  }
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return FDTD_OK;
 }
@@ -737,8 +819,17 @@ fdtd_status fdtd_get_dft(fdtd_handle* h, int32_t monitor_id, double* re, double*
 
 fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6) {
   if (!h || !scale6) return FDTD_ERR_INVALID_ARG;
-  if (h->desc.storage == FDTD_STORE_F32) return FDTD_OK;
-  return fail(h, FDTD_ERR_UNSUPPORTED, "reduced-precision storage is not built");
+  for (int c = 0; c < 6; ++c)
+    if (!(scale6[c] > 0.0f) || !std::isfinite(scale6[c]))
+      return fail(h, FDTD_ERR_INVALID_ARG, "storage scale %d must be positive and finite", c);
+  if (h->esz != 2) return FDTD_OK;  // FP32 / FP64 storage is unscaled
+  for (int c = 0; c < 6; ++c) {
+    const int e = (int)std::lround(std::log2((double)scale6[c]));
+    if (e < -100 || e > 100) return fail(h, FDTD_ERR_INVALID_ARG, "storage scale out of range");
+    h->scale[c] = std::ldexp(1.0f, e);
+    h->inv_scale[c] = std::ldexp(1.0f, -e);
+  }
+  return FDTD_OK;
 }
 
 fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out6) {
@@ -749,6 +840,339 @@ fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out6) {
   out6[3] = h->cfg.z_chunks;
   out6[4] = h->last_launches;
   out6[5] = h->cfg.min_blocks;
+  return FDTD_OK;
+}
+
+}  // extern "C"
+
+// ============================================================================== batches
+
+struct fdtd_batch {
+  std::vector<fdtd_handle*> sims;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int storage = 0, esz = 4;
+  fdtd::TiledConfig cfg{0, 0, 1, 64};
+  bool cfg_ready = false;
+  fdtd::TiledArgs* d_args = nullptr;  // [2][n]
+  fdtd::TiledArgs* h_args = nullptr;  // pinned staging [2][n]
+  std::map<int, std::pair<int4*, int>> items;  // per BLT: device work items, count
+  unsigned int* d_counters = nullptr;
+  int counters_cap = 0;
+  int ctas = 0;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<long long> gkey;
+  int last_launches = 0, last_graph = 0;
+  std::string err;
+};
+
+namespace {
+
+fdtd_status bfail(fdtd_batch* b, fdtd_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (b) b->err = buf; else g_create_error = buf;
+  return s;
+}
+
+#define BCUDA(b, call)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return bfail((b), e_ == cudaErrorMemoryAllocation ? FDTD_ERR_OOM : FDTD_ERR_CUDA,   \
+                   "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,       \
+                   __LINE__);                                                             \
+  } while (0)
+
+fdtd::TiledConfig batch_cfg(const fdtd_batch* b, int blt, int rows) {
+  fdtd::TiledConfig c{blt, rows, 1, 64, 1, b->storage, b->esz};
+  return c;
+}
+
+// Work items of one BLT value: every tile column of every simulation (one z-chunk: the whole
+// column is one item), longest z-march first so the queue's tail is short.
+fdtd_status batch_items(fdtd_batch* b, const fdtd::TiledConfig& c, std::pair<int4*, int>* out) {
+  const int key = c.blt * 100 + c.rows;
+  auto it = b->items.find(key);
+  if (it != b->items.end()) {
+    *out = it->second;
+    return FDTD_OK;
+  }
+  std::vector<std::pair<int, int4>> v;
+  for (size_t i = 0; i < b->sims.size(); ++i) {
+    const Grid& g = b->sims[i]->g;
+    const dim3 gd = fdtd::tiled2_grid(c, g);
+    for (unsigned by = 0; by < gd.y; ++by)
+      for (unsigned bx = 0; bx < gd.x; ++bx)
+        v.push_back({g.nz, make_int4((int)i, (int)bx, (int)by, 0)});
+  }
+  std::stable_sort(v.begin(), v.end(),
+                   [](const std::pair<int, int4>& a, const std::pair<int, int4>& b2) {
+                     return a.first > b2.first;
+                   });
+  std::vector<int4> host(v.size());
+  for (size_t i = 0; i < v.size(); ++i) host[i] = v[i].second;
+  int4* d = nullptr;
+  BCUDA(b, cudaMalloc(&d, host.size() * sizeof(int4)));
+  BCUDA(b, cudaMemcpy(d, host.data(), host.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  b->items[key] = {d, (int)host.size()};
+  *out = b->items[key];
+  return FDTD_OK;
+}
+
+fdtd_status batch_maps(fdtd_batch* b, int rows) {
+  for (fdtd_handle* h : b->sims) {
+    fdtd_status s = ensure_maps(h, 64, rows);
+    if (s != FDTD_OK) return bfail(b, s, "sim: %s", h->err.c_str());
+  }
+  return FDTD_OK;
+}
+
+// Fills h_args [2][n] for config c: parity p reads field set (cur ^ p) of each simulation.
+void batch_fill_args(fdtd_batch* b, const fdtd::TiledConfig& c, bool with_io) {
+  const size_t n = b->sims.size();
+  for (size_t i = 0; i < n; ++i) {
+    fdtd_handle* h = b->sims[i];
+    fdtd::TiledConfig ci = c;
+    ci.z_chunks = 1;
+    for (int p = 0; p < 2; ++p)
+      b->h_args[p * n + i] = make_tiled_args(h, ci, h->t, with_io, h->cur ^ p);
+  }
+}
+
+fdtd_status batch_counters(fdtd_batch* b, int need) {
+  if (need <= b->counters_cap) return FDTD_OK;
+  if (b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+    b->gkey.clear();
+  }
+  cudaFree(b->d_counters);
+  b->d_counters = nullptr;
+  const int cap = std::max(need, 2 * b->counters_cap);
+  BCUDA(b, cudaMalloc(&b->d_counters, cap * sizeof(unsigned int)));
+  b->counters_cap = cap;
+  return FDTD_OK;
+}
+
+fdtd_status batch_launch(fdtd_batch* b, const fdtd::TiledConfig& c, int flip, long long t_off,
+                         unsigned int* counter, cudaStream_t st) {
+  std::pair<int4*, int> it;
+  fdtd_status s = batch_items(b, c, &it);
+  if (s != FDTD_OK) return s;
+  fdtd::BatchArgs a;
+  a.grids = b->d_args;
+  a.ngrids = (int)b->sims.size();
+  a.flip = flip;
+  a.t_offset = t_off;
+  a.items = it.first;
+  a.nitems = it.second;
+  a.counter = counter;
+  BCUDA(b, fdtd::launch_tiled2_batch(c, a, b->ctas, st));
+  return FDTD_OK;
+}
+
+fdtd_status batch_autotune(fdtd_batch* b, cudaStream_t st) {
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+  std::vector<fdtd::TiledConfig> cands;
+  for (int rows : {16, 8})
+    for (int blt = 1; blt <= 4; ++blt) {
+      fdtd::TiledConfig c = batch_cfg(b, blt, rows);
+      if (fdtd::tiled2_batch_supported(c)) cands.push_back(c);
+    }
+  fdtd_status s = batch_counters(b, 4);
+  if (s != FDTD_OK) return s;
+  cudaEvent_t e0, e1;
+  BCUDA(b, cudaEventCreate(&e0));
+  BCUDA(b, cudaEventCreate(&e1));
+  float best = 1e30f;
+  fdtd::TiledConfig best_c = cands[0];
+  int best_ctas = nsm;
+  for (int pass = 0; pass < 2; ++pass)  // the first pass also brings the clocks up
+    for (const auto& c : cands) {
+      if ((s = batch_maps(b, c.rows)) != FDTD_OK) return s;
+      b->ctas = nsm * fdtd::tiled2_batch_ctas_per_sm(c);
+      batch_fill_args(b, c, false);
+      BCUDA(b, cudaMemcpyAsync(b->d_args, b->h_args, 2 * b->sims.size() * sizeof(fdtd::TiledArgs),
+                               cudaMemcpyHostToDevice, st));
+      BCUDA(b, cudaMemsetAsync(b->d_counters, 0, 3 * sizeof(unsigned int), st));
+      if ((s = batch_launch(b, c, 0, 0, b->d_counters, st)) != FDTD_OK) return s;
+      BCUDA(b, cudaEventRecord(e0, st));
+      for (int r = 1; r < 3; ++r)
+        if ((s = batch_launch(b, c, 0, 0, b->d_counters + r, st)) != FDTD_OK) return s;
+      BCUDA(b, cudaEventRecord(e1, st));
+      BCUDA(b, cudaEventSynchronize(e1));
+      float ms = 0;
+      BCUDA(b, cudaEventElapsedTime(&ms, e0, e1));
+      const float per_step = ms / (2 * c.blt);
+      if (pass == 1 && per_step < best) {
+        best = per_step;
+        best_c = c;
+        best_ctas = b->ctas;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->cfg = best_c;
+  b->ctas = best_ctas;
+  b->cfg_ready = true;
+  return FDTD_OK;
+}
+
+// Makes `waiter` wait for everything queued on `on`.
+fdtd_status stream_after(fdtd_batch* b, cudaStream_t waiter, cudaStream_t on) {
+  if (waiter == on) return FDTD_OK;
+  cudaEvent_t ev;
+  BCUDA(b, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  BCUDA(b, cudaEventRecord(ev, on));
+  BCUDA(b, cudaStreamWaitEvent(waiter, ev, 0));
+  cudaEventDestroy(ev);
+  return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fdtd_batch_last_error(const fdtd_batch* b) {
+  return b ? b->err.c_str() : g_create_error.c_str();
+}
+
+fdtd_status fdtd_batch_create(fdtd_handle* const* sims, int32_t n, fdtd_batch** out) {
+  if (!sims || !out || n < 1) return bfail(nullptr, FDTD_ERR_INVALID_ARG, "empty batch");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    const fdtd_handle* h = sims[i];
+    if (!h) return bfail(nullptr, FDTD_ERR_INVALID_ARG, "simulation %d is NULL", i);
+    if (h->desc.device != sims[0]->desc.device || h->storage != sims[0]->storage)
+      return bfail(nullptr, FDTD_ERR_INVALID_ARG, "simulations must share device and storage");
+    if (h->storage == FDTD_STORE_F64)
+      return bfail(nullptr, FDTD_ERR_UNSUPPORTED, "FP64 storage has no batched kernel");
+    if (h->coef_mode != kCoefMaterial)
+      return bfail(nullptr, FDTD_ERR_UNSUPPORTED,
+                   "simulation %d has no material map (coefficients not set or too many)", i);
+  }
+  fdtd_batch* b = new fdtd_batch();
+  b->sims.assign(sims, sims + n);
+  b->device = sims[0]->desc.device;
+  b->storage = sims[0]->storage;
+  b->esz = sims[0]->esz;
+  DeviceGuard dg(b->device);
+  const size_t bytes = 2 * (size_t)n * sizeof(fdtd::TiledArgs);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&b->d_args, bytes) != cudaSuccess ||
+      cudaMallocHost(&b->h_args, bytes) != cudaSuccess) {
+    fdtd_batch_destroy(b);
+    return bfail(nullptr, FDTD_ERR_OOM, "batch allocation failed");
+  }
+  *out = b;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_destroy(fdtd_batch* b) {
+  if (!b) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  for (auto& kv : b->items) cudaFree(kv.second.first);
+  cudaFree(b->d_counters);
+  cudaFree(b->d_args);
+  if (b->h_args) cudaFreeHost(b->h_args);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* stream) {
+  if (!b || T < 0) return FDTD_ERR_INVALID_ARG;
+  if (T == 0) return FDTD_OK;
+  DeviceGuard dg(b->device);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+  fdtd_status s;
+  for (fdtd_handle* h : b->sims) {
+    if ((s = ensure_tables(h, h->t + T)) != FDTD_OK) return bfail(b, s, "%s", h->err.c_str());
+    if ((s = stream_after(b, st, h->stream)) != FDTD_OK) return s;
+  }
+  if (!b->cfg_ready && (s = batch_autotune(b, st)) != FDTD_OK) return s;
+  const fdtd::TiledConfig c = b->cfg;
+  const long long nfull = T / c.blt;
+  const int rem = (int)(T % c.blt);
+  const int nl = (int)nfull + (rem ? 1 : 0);
+  if ((s = batch_maps(b, c.rows)) != FDTD_OK) return s;
+  if ((s = batch_counters(b, nl)) != FDTD_OK) return s;
+  std::pair<int4*, int> tmp;
+  if ((s = batch_items(b, c, &tmp)) != FDTD_OK) return s;
+  if (rem && (s = batch_items(b, batch_cfg(b, rem, c.rows), &tmp)) != FDTD_OK) return s;
+  batch_fill_args(b, c, true);
+
+  auto record = [&](cudaStream_t rs) -> fdtd_status {
+    BCUDA(b, cudaMemcpyAsync(b->d_args, b->h_args,
+                             2 * b->sims.size() * sizeof(fdtd::TiledArgs),
+                             cudaMemcpyHostToDevice, rs));
+    BCUDA(b, cudaMemsetAsync(b->d_counters, 0, nl * sizeof(unsigned int), rs));
+    for (int k = 0; k < nl; ++k) {
+      const fdtd::TiledConfig ck = (k < nfull) ? c : batch_cfg(b, rem, c.rows);
+      fdtd_status r = batch_launch(b, ck, k & 1, (long long)k * c.blt, b->d_counters + k, rs);
+      if (r != FDTD_OK) return r;
+    }
+    return FDTD_OK;
+  };
+
+  b->last_graph = 0;
+  if (use_graph) {
+    std::vector<long long> key = {T, c.blt, c.rows, b->ctas};
+    for (fdtd_handle* h : b->sims) {
+      key.push_back(h->t);
+      key.push_back(h->cur);
+    }
+    if (!b->gexec || key != b->gkey) {
+      if (b->gexec) {
+        cudaGraphExecDestroy(b->gexec);
+        b->gexec = nullptr;
+      }
+      cudaGraph_t graph;
+      BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
+      fdtd_status r = record(b->stream);
+      cudaError_t ce = cudaStreamEndCapture(b->stream, &graph);
+      if (r != FDTD_OK) return r;
+      if (ce != cudaSuccess) return bfail(b, FDTD_ERR_CUDA, "graph capture failed: %s",
+                                          cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&b->gexec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return bfail(b, FDTD_ERR_CUDA, "graph instantiation failed: %s",
+                                          cudaGetErrorString(ce));
+      b->gkey = key;
+    } else {
+      b->last_graph = 1;
+    }
+    BCUDA(b, cudaGraphLaunch(b->gexec, st));
+  } else {
+    if ((s = record(st)) != FDTD_OK) return s;
+  }
+  for (fdtd_handle* h : b->sims) {
+    h->t += T;
+    h->cur ^= (nl & 1);
+    h->last_kernel = FDTD_KERNEL_TILED_W64;
+    h->last_launches = nl;
+    if ((s = stream_after(b, h->stream, st)) != FDTD_OK) return s;
+  }
+  b->last_launches = nl;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_get_config(const fdtd_batch* b, int32_t* out6) {
+  if (!b || !out6) return FDTD_ERR_INVALID_ARG;
+  out6[0] = b->cfg.blt;
+  out6[1] = b->cfg.rows;
+  out6[2] = b->ctas;
+  auto it = b->items.find(b->cfg.blt * 100 + b->cfg.rows);
+  out6[3] = it == b->items.end() ? 0 : it->second.second;
+  out6[4] = b->last_launches;
+  out6[5] = b->last_graph;
   return FDTD_OK;
 }
 

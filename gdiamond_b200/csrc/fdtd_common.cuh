@@ -69,6 +69,20 @@ __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 
+// FP32 -> BF16 bit pattern, round to nearest even on the FP32 bits (subnormals included, NaN
+// kept quiet).  Defined here rather than taken from a conversion instruction so the rounding
+// of stored fields is specified exactly, the same on the device and in the oracle.
+__host__ __device__ __forceinline__ uint16_t bf16_rne_bits(float x) {
+#ifdef __CUDA_ARCH__
+  const uint32_t b = __float_as_uint(x);
+#else
+  uint32_t b;
+  __builtin_memcpy(&b, &x, 4);
+#endif
+  if ((b & 0x7FFFFFFFu) > 0x7F800000u) return (uint16_t)((b >> 16) | 0x0040u);
+  return (uint16_t)((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16);
+}
+
 // new = Ca*old + Cb*curl
 __device__ __forceinline__ float yee(float ca, float old, float cb, float curl) {
   return add(mul(ca, old), mul(cb, curl));

@@ -11,10 +11,20 @@ struct FieldPtrs {
 };
 
 // ---------------------------------------------------------------- naive kernels
+// fp64: fields are double (FP64 storage), else float.
 cudaError_t launch_naive_step(const Grid& g, const FieldPtrs& F, const float* const* coef,
                               const uint16_t* mat, const Material* tab, const Sources& S,
                               const Monitors& M, long long t, float dx, cudaStream_t st,
-                              int* launches);
+                              int* launches, bool fp64);
+
+// ---------------------------------------------------------------- storage conversion
+// Pitched field array of `storage` (0 FP32, 1 FP16, 2 BF16, 3 FP64) <-> pitched FP32 / FP64.
+cudaError_t convert_field_to_f32(const Grid& g, const void* src, int storage, float scale,
+                                 float* dst, cudaStream_t st);
+cudaError_t convert_field_from_f32(const Grid& g, const float* src, int storage, float inv_scale,
+                                   void* dst, cudaStream_t st);
+cudaError_t convert_field_to_f64(const Grid& g, const void* src, int storage, float scale,
+                                 double* dst, cudaStream_t st);
 
 // ---------------------------------------------------------------- tiled kernel
 struct TiledArgs {
@@ -29,6 +39,20 @@ struct TiledArgs {
   float dx;
   int zlen;               // output planes per z-chunk
   int* err;               // device error word
+  float scale[6];         // 16-bit storage: value = stored * scale (powers of two)
+  float inv_scale[6];
+};
+
+// A batch of grids for the persistent kernel: per-grid arguments (tensor maps included) in
+// device memory, and the (grid, bx, by, bz) work items pulled through an atomic counter.
+struct BatchArgs {
+  const TiledArgs* grids;  // [2][ngrids]: the arguments of each grid for both ping-pong parities
+  int ngrids;
+  int flip;                // parity of this launch: grids[flip * ngrids + g] is used
+  long long t_offset;      // added to each grid's t0 (steps since the batch run started)
+  const int4* items;       // (grid, bx, by, bz), longest z-march first
+  int nitems;
+  unsigned int* counter;   // zero before the launch
 };
 
 struct TiledConfig {
@@ -37,6 +61,8 @@ struct TiledConfig {
   int z_chunks;   // z-chunks per tile column
   int width = 32; // cells per warp row: 32 (k_tiled.cu) or 64 (k_tiled2.cu, x-pairs)
   int min_blocks = 1;  // register cap: CTAs per SM the compiler must fit (x-pair family)
+  int storage = 0;     // 0 FP32, 1 FP16, 2 BF16 (x-pair family only for 16-bit)
+  int esz = 4;         // bytes per stored field value
 };
 
 // Tile geometry shared by the host (grid size, tensor-map boxes) and the kernel.
@@ -46,14 +72,27 @@ __host__ __device__ constexpr int tiled_sy(int blt, int rows) { return rows - 2 
 constexpr int kTiledStages = 3;
 constexpr int kMatBoxX = 40;  // material box is widened to start on an 8-element boundary
 
-// Two-cells-per-thread family (k_tiled2.cu): 64-wide warp rows.
-__host__ __device__ constexpr int tiled2_sx(int blt) { return 4 * ((64 - 2 * blt) / 4); }
-constexpr int kTiled2Stages = 2;
-constexpr int kMatBoxX2 = 72;  // 64 + 4 alignment offset, rounded to a 16-byte row
+// Two-cells-per-thread family (k_tiled2.cu): 64-wide warp rows.  x tile starts are multiples
+// of 16 bytes of the stored type: al = 16 / esz elements.
+__host__ __device__ constexpr int tiled2_align(int esz) { return 16 / esz; }
+__host__ __device__ constexpr int tiled2_sx(int blt, int esz) {
+  return tiled2_align(esz) * ((64 - 2 * blt) / tiled2_align(esz));
+}
+__host__ __device__ constexpr int tiled2_xbase(int blt, int esz) {
+  return -tiled2_align(esz) * ((blt + tiled2_align(esz) - 1) / tiled2_align(esz));
+}
+constexpr int kTiled2Stages = 2;  // FP32; 16-bit storage uses one more
+constexpr int kMatBoxX2 = 72;     // 64 + 4 alignment offset, rounded to a 16-byte row
 bool tiled2_config_supported(const TiledConfig& c);
 dim3 tiled2_grid(const TiledConfig& c, const Grid& g);
 cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& args, const Grid& g,
                           cudaStream_t st);
+// Persistent batch form (ROWS 8 or 16).
+bool tiled2_batch_supported(const TiledConfig& c);
+size_t tiled2_batch_smem(const TiledConfig& c);
+int tiled2_batch_ctas_per_sm(const TiledConfig& c);
+cudaError_t launch_tiled2_batch(const TiledConfig& c, const BatchArgs& b, int ctas,
+                                cudaStream_t st);
 
 bool tiled_config_supported(const TiledConfig& c);
 size_t tiled_smem_bytes(const TiledConfig& c);

@@ -1,14 +1,29 @@
-// k_tiled2.cu -- the z-streaming temporally tiled Yee kernel with two cells per thread in x.
+// k_tiled2.cu -- the z-streaming temporally tiled Yee kernel with two cells per thread in x,
+// for one grid (fdtd_tiled2) and for a batch of independent grids in one persistent launch
+// (fdtd_tiled2_batch).
 //
 // Same schedule as k_tiled.cu (TMA plane pipeline, BLT-level (z,t) wavefront, trapezoid tiles in
-// x and y, material map, fused FP64 DFT, bounded waits, bit-exact arithmetic), but each thread
-// owns an x-pair (2l, 2l+1) of a 64-wide warp row:
+// x and y, material map, fused FP64 DFT, bounded waits), but each thread owns an x-pair
+// (2l, 2l+1) of a 64-wide warp row:
 //  * the pair's inner neighbours are in registers; only the pair edges cross lanes, so a level
 //    needs one shuffle per field direction per pair instead of per cell;
-//  * staged planes, y-exchange planes and outputs move as float2 (one shared/global instruction
+//  * staged planes, y-exchange planes and outputs move as pairs (one shared/global instruction
 //    for two cells);
 //  * the x-trapezoid wastes 2*BLT of 64 columns instead of 2*BLT of 32;
-//  * monitor planes are tested once per z-iteration against a precomputed plane range.
+//  * source and monitor planes are tested once per z-iteration against CTA-uniform ranges.
+//
+// Field storage S is float, __half or __nv_bfloat16.  Arithmetic is FP32 in every case and the
+// intermediate time levels never leave the SM in reduced precision: only the HBM round trip of
+// each BLT-step pass is 16-bit.  A 16-bit value v is stored as v * inv_scale[c] and read back
+// times scale[c]; scales are powers of two, so the scaling itself rounds nothing.  With FP32
+// storage no scaling is applied and every multiply/add is separately rounded: results are
+// bit-identical to the reference CPU update.
+//
+// x tile starts are multiples of 16 bytes of the stored type (4 floats, 8 halves): the TMA rule
+// for the innermost coordinate.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "fdtd_kernels.cuh"
 
 namespace fdtd {
@@ -18,16 +33,61 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr long long kWaitLimit = 2000000000LL;  // SM clocks, about one second
 
-template <int B, int TY>
+template <typename S>
+struct Store;
+
+template <>
+struct Store<float> {
+  static constexpr bool kScaled = false;
+  __device__ static float2 ld2(const float* p, float) {
+    return *reinterpret_cast<const float2*>(p);
+  }
+  __device__ static void st2(float* p, float a, float b, float) {
+    *reinterpret_cast<float2*>(p) = make_float2(a, b);
+  }
+  __device__ static void st1(float* p, float a, float) { *p = a; }
+};
+
+template <>
+struct Store<__half> {
+  static constexpr bool kScaled = true;
+  __device__ static float2 ld2(const __half* p, float sc) {
+    const float2 v = __half22float2(*reinterpret_cast<const __half2*>(p));
+    return make_float2(v.x * sc, v.y * sc);
+  }
+  __device__ static void st2(__half* p, float a, float b, float inv) {
+    *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a * inv, b * inv);
+  }
+  __device__ static void st1(__half* p, float a, float inv) { *p = __float2half_rn(a * inv); }
+};
+
+template <>
+struct Store<__nv_bfloat16> {
+  static constexpr bool kScaled = true;
+  __device__ static float2 ld2(const __nv_bfloat16* p, float sc) {
+    const float2 v = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+    return make_float2(v.x * sc, v.y * sc);
+  }
+  __device__ static void st2(__nv_bfloat16* p, float a, float b, float inv) {
+    const uint32_t lo = bf16_rne_bits(a * inv), hi = bf16_rne_bits(b * inv);
+    *reinterpret_cast<uint32_t*>(p) = lo | (hi << 16);
+  }
+  __device__ static void st1(__nv_bfloat16* p, float a, float inv) {
+    *reinterpret_cast<uint16_t*>(p) = bf16_rne_bits(a * inv);
+  }
+};
+
+template <typename S, int B, int TY>
 struct Tiled2 {
+  static constexpr int ESZ = (int)sizeof(S);
   static constexpr int W = 64;                 // cells per warp row
   static constexpr int PL = W * TY;            // elements of one staged field plane
   static constexpr int MPL = kMatBoxX2 * TY;   // elements of one staged material plane
-  static constexpr int NS = kTiled2Stages;
-  static constexpr int SX = tiled2_sx(B);
+  static constexpr int NS = ESZ == 4 ? kTiled2Stages : kTiled2Stages + 1;
+  static constexpr int SX = tiled2_sx(B, ESZ);
   static constexpr int SY = tiled_sy(B, TY);
-  static constexpr int XBASE = tiled_xbase(B);
-  static constexpr uint32_t STAGE_F_BYTES = 6u * PL * 4u;
+  static constexpr int XBASE = tiled2_xbase(B, ESZ);
+  static constexpr uint32_t STAGE_F_BYTES = 6u * PL * ESZ;
   static constexpr uint32_t STAGE_M_BYTES = MPL * 2u;
   static constexpr uint32_t TX_BYTES = STAGE_F_BYTES + STAGE_M_BYTES;
   static constexpr size_t OFF_M = (size_t)NS * STAGE_F_BYTES;
@@ -36,45 +96,55 @@ struct Tiled2 {
   static constexpr size_t OFF_BAR = OFF_E + (size_t)B * 2u * PL * 4u;
   static constexpr size_t SMEM = OFF_BAR + NS * 8u + 128u;  // + alignment slack
   static_assert(SY >= 1, "tile too short for this BLT");
-  static_assert(STAGE_M_BYTES % 128 == 0, "stage alignment");
+  static_assert(STAGE_M_BYTES % 128 == 0 && (PL * ESZ) % 128 == 0, "stage alignment");
 };
 
 struct Pair {
   float a, b;  // even cell, odd cell
 };
 
-__device__ __forceinline__ float2 ld2(const float* p) { return *reinterpret_cast<const float2*>(p); }
-__device__ __forceinline__ void st2(float* p, float a, float b) {
+__device__ __forceinline__ float2 ldf2(const float* p) {
+  return *reinterpret_cast<const float2*>(p);
+}
+__device__ __forceinline__ void stf2(float* p, float a, float b) {
   *reinterpret_cast<float2*>(p) = make_float2(a, b);
 }
 
-// MINB > 1 caps registers so that MINB CTAs fit on an SM (more warps to hide latency, at the
-// cost of some spilled state); the autotuner decides per grid whether that pays.
-template <int B, int TY, int MINB>
-__global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_constant__ TiledArgs a) {
-  using K = Tiled2<B, TY>;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  float* st_f = reinterpret_cast<float*>(smem);
-  uint16_t* st_m = reinterpret_cast<uint16_t*>(smem + K::OFF_M);
-  float* hbuf = reinterpret_cast<float*>(smem + K::OFF_H);  // [2][Hz,Hx][PL]
-  float* ebuf = reinterpret_cast<float*>(smem + K::OFF_E);  // [B][Ex,Ez][PL]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + K::OFF_BAR);
-  __shared__ int s_abort;
+// Shared-memory carve-up of one CTA (all tiles it processes reuse it).
+struct Smem {
+  unsigned char* base;
+  uint64_t* bars;
+  int* abort;
+};
+
+// Runs the z-march of one tile (tile column (bx, by), z-chunk bz) of the grid described by `a`.
+// `gbase` counts the pipeline stages this CTA consumed before (mbarrier phases continue across
+// tiles in the persistent form).  Every thread of the CTA calls it; returns false when a
+// bounded wait expired (the CTA must then stop).
+template <typename S, int B, int TY>
+__device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz,
+                                      const Smem& sm, uint32_t& gbase, long long t_offset) {
+  using K = Tiled2<S, B, TY>;
+  using St = Store<S>;
+  S* st_f = reinterpret_cast<S*>(sm.base);
+  uint16_t* st_m = reinterpret_cast<uint16_t*>(sm.base + K::OFF_M);
+  float* hbuf = reinterpret_cast<float*>(sm.base + K::OFF_H);  // [2][Hz,Hx][PL]
+  float* ebuf = reinterpret_cast<float*>(sm.base + K::OFF_E);  // [B][Ex,Ez][PL]
+  uint64_t* bars = sm.bars;
 
   const Grid g = a.g;
-  const int z0 = (int)blockIdx.z * a.zlen;
-  if (z0 >= g.nz) return;  // uniform across the CTA
+  const int z0 = bz * a.zlen;
+  if (z0 >= g.nz) return true;  // uniform across the CTA
   const int z1 = min(g.nz, z0 + a.zlen);
   const int ps = z0 - B;
   const int niter = (z1 - z0) + 2 * B;
 
   const int lx = threadIdx.x, ly = threadIdx.y;
   const int tid = ly * 32 + lx;
-  const int X = (int)blockIdx.x * K::SX + K::XBASE;  // multiple of 4
-  const int Y = (int)blockIdx.y * K::SY - B;
+  const int X = bx * K::SX + K::XBASE;  // multiple of 16 bytes of S
+  const int Y = by * K::SY - B;
   const int X8 = X & ~7;
-  const int cx0 = 2 * lx;                            // tile column of the even cell
+  const int cx0 = 2 * lx;               // tile column of the even cell
   const int x0 = X + cx0, x1 = x0 + 1, y = Y + ly;
   const bool row_int = y >= 1 && y <= g.ny - 2;
   const bool int0 = row_int && x0 >= 1 && x0 <= g.nx - 2;
@@ -103,26 +173,29 @@ __global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_consta
     mon_lo = min(mon_lo, k);
     mon_hi = max(mon_hi, k + B - 1);
   }
-
-  if (tid == 0) {
-    s_abort = 0;
-    for (int s = 0; s < K::NS; ++s) mbar_init(&bars[s], 1);
-    fence_mbar_init();
+  float sc[6], inv[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    sc[c] = St::kScaled ? a.scale[c] : 1.0f;
+    inv[c] = St::kScaled ? a.inv_scale[c] : 1.0f;
   }
+
   for (int q = tid; q < (4 + 2 * B) * K::PL; q += 32 * TY) hbuf[q] = 0.0f;
-  __syncthreads();
+  __syncthreads();  // zeroed exchange planes; the previous tile's stages are all consumed
 
   auto issue = [&](int it_) {
-    const int stage = it_ % K::NS;
+    const uint32_t u = gbase + (uint32_t)it_;
+    const int stage = (int)(u % K::NS);
     uint64_t* bar = &bars[stage];
     mbar_arrive_expect_tx(bar, K::TX_BYTES);
-    float* d = st_f + stage * 6 * K::PL;
+    S* d = st_f + stage * 6 * K::PL;
     const int pz = ps + it_;
 #pragma unroll
     for (int c = 0; c < 6; ++c) tma_load_3d(d + c * K::PL, &a.tm_src[c], bar, X, Y, pz);
     tma_load_3d(st_m + stage * K::MPL, &a.tm_mat, bar, X8, Y, pz);
   };
   if (tid == 0) {
+    fence_proxy_async_smem();
     for (int it_ = 0; it_ < K::NS && it_ < niter; ++it_) issue(it_);
   }
 
@@ -142,40 +215,43 @@ __global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_consta
   const int om = ly * kMatBoxX2 + cx0 + (X - X8);  // even: a 4-byte aligned id pair
   const float dx = a.dx;
   const long long pitch = g.pitch, plane = g.plane;
+  S* const* dst = reinterpret_cast<S* const*>(a.dst.f);
 
   int it = 0;
   bool abort = false;
   for (; it < niter; ++it) {
     const int p = ps + it;
-    const int stage = it % K::NS;
-    if (!mbar_wait_bounded(&bars[stage], (uint32_t)(it / K::NS) & 1u, kWaitLimit)) {
-      s_abort = 1;
+    const uint32_t u = gbase + (uint32_t)it;
+    const int stage = (int)(u % K::NS);
+    if (!mbar_wait_bounded(&bars[stage], (u / K::NS) & 1u, kWaitLimit)) {
+      *sm.abort = 1;
       atomicExch(a.err, kErrTimeout);
     }
     if (B == 1) __syncthreads();  // orders last iteration's ebuf writes before this read
     const bool mon_iter = p >= mon_lo && p <= mon_hi;
     const bool src_iter = smask != 0 && p >= src_lo && p <= src_hi;
 
-    const float* S0 = st_f + stage * 6 * K::PL;
+    const S* S0 = st_f + stage * 6 * K::PL;
 #pragma unroll
     for (int s = B; s >= 1; --s) mq[s] = mq[s - 1];
     mq[0] = *reinterpret_cast<const uint32_t*>(st_m + stage * K::MPL + om);
     Pair Hc[3], Eo[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float2 hv = ld2(S0 + (3 + c) * K::PL + o);
-      const float2 ev = ld2(S0 + c * K::PL + o);
+      const float2 hv = St::ld2(S0 + (3 + c) * K::PL + o, sc[3 + c]);
+      const float2 ev = St::ld2(S0 + c * K::PL + o, sc[c]);
       Hc[c] = Pair{hv.x, hv.y};
       Eo[c] = Pair{ev.x, ev.y};
     }
-    float2 hz_ym = ld2(S0 + 5 * K::PL + oym), hx_ym = ld2(S0 + 3 * K::PL + oym);
+    float2 hz_ym = St::ld2(S0 + 5 * K::PL + oym, sc[5]);
+    float2 hx_ym = St::ld2(S0 + 3 * K::PL + oym, sc[3]);
     Pair EnPrev[3] = {};
     Pair EnB[3] = {}, HnB[3] = {};
 
 #pragma unroll
     for (int s = 1; s <= B; ++s) {
       const int e = p - s + 1;
-      const long long t = a.t0 + (s - 1);
+      const long long t = a.t0 + t_offset + (s - 1);
       // ---------------- E^s(e)
       // x-1 neighbour: odd cell of lane-1 for the even cell, own even cell for the odd cell
       const float hz_xm = __shfl_up_sync(kFull, Hc[2].b, 1);
@@ -188,8 +264,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_consta
       czp.a = sub(sub(Hc[1].a, hy_xm), sub(Hc[0].a, hx_ym.x));
       czp.b = sub(sub(Hc[1].b, Hc[1].a), sub(Hc[0].b, hx_ym.y));
       Pair En[3] = {Eo[0], Eo[1], Eo[2]};
-      const bool zint_e = e >= 1 && e <= g.nz - 2;
-      if (zint_e) {
+      if (e >= 1 && e <= g.nz - 2) {
         if (src_iter) {
           float v;
           if (source_value(a.S, 0, x0, y, e, t, &v)) cxp.a = sub(cxp.a, mul(v, dx));
@@ -219,7 +294,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_consta
       const float ez_xp = __shfl_down_sync(kFull, Ep[s][2].a, 1);
       const float ey_xp = __shfl_down_sync(kFull, Ep[s][1].a, 1);
       float* eb = ebuf + (s - 1) * 2 * K::PL;
-      const float2 ex_yp = ld2(eb + oyp), ez_yp = ld2(eb + K::PL + oyp);
+      const float2 ex_yp = ldf2(eb + oyp), ez_yp = ldf2(eb + K::PL + oyp);
       cxp.a = sub(sub(En[1].a, Ep[s][1].a), sub(ez_yp.x, Ep[s][2].a));
       cxp.b = sub(sub(En[1].b, Ep[s][1].b), sub(ez_yp.y, Ep[s][2].b));
       cyp.a = sub(sub(Ep[s][2].b, Ep[s][2].a), sub(En[0].a, Ep[s][0].a));
@@ -227,8 +302,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_consta
       czp.a = sub(sub(ex_yp.x, Ep[s][0].a), sub(Ep[s][1].b, Ep[s][1].a));
       czp.b = sub(sub(ex_yp.y, Ep[s][0].b), sub(ey_xp, Ep[s][1].b));
       Pair Hn[3] = {Hp[s - 1][0], Hp[s - 1][1], Hp[s - 1][2]};
-      const bool zint_h = e - 1 >= 1 && e - 1 <= g.nz - 2;
-      if (zint_h) {
+      if (e - 1 >= 1 && e - 1 <= g.nz - 2) {
         if (src_iter) {
           float v;
           if (source_value(a.S, 3, x0, y, e - 1, t, &v)) cxp.a = sub(cxp.a, mul(v, dx));
@@ -253,7 +327,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_consta
           Hn[2].b = yee(c1.z, Hp[s - 1][2].b, c1.w, czp.b);
         }
       }
-      // ---------------- running DFT
+      // ---------------- running DFT (of the FP32 values, before any storage rounding)
       if (mon_iter && (out0 || out1)) {
         for (int n = 0; n < a.M.n; ++n) {
           const MonitorDev& m = a.M.m[n];
@@ -270,16 +344,16 @@ __global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_consta
       // ---------------- exchange
       if (s < B) {
         float* hb = hbuf + (s & 1) * 2 * K::PL;
-        st2(hb + o, Hn[2].a, Hn[2].b);
-        st2(hb + K::PL + o, Hn[0].a, Hn[0].b);
+        stf2(hb + o, Hn[2].a, Hn[2].b);
+        stf2(hb + K::PL + o, Hn[0].a, Hn[0].b);
       }
       __syncthreads();
-      st2(eb + o, En[0].a, En[0].b);
-      st2(eb + K::PL + o, En[2].a, En[2].b);
+      stf2(eb + o, En[0].a, En[0].b);
+      stf2(eb + K::PL + o, En[2].a, En[2].b);
       if (s == 1) {
-        abort = s_abort != 0;
+        abort = *sm.abort != 0;
         if (!abort && tid == 0 && it + K::NS < niter) {
-          fence_proxy_async_smem();
+          fence_proxy_async_smem();  // generic-proxy reads of this stage precede the refill
           issue(it + K::NS);
         }
       }
@@ -295,8 +369,8 @@ __global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_consta
       }
       if (s < B) {
         const float* hb = hbuf + (s & 1) * 2 * K::PL;
-        hz_ym = ld2(hb + oym);
-        hx_ym = ld2(hb + K::PL + oym);
+        hz_ym = ldf2(hb + oym);
+        hx_ym = ldf2(hb + K::PL + oym);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           Hc[c] = Hn[c];
@@ -323,78 +397,222 @@ __global__ void __launch_bounds__(32 * TY, MINB) fdtd_tiled2(const __grid_consta
         const long long idx = x0 + (long long)y * pitch + (long long)eB * plane;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          if (both) st2(a.dst.f[c] + idx, EnB[c].a, EnB[c].b);
-          else if (out0) a.dst.f[c][idx] = EnB[c].a;
-          else a.dst.f[c][idx + 1] = EnB[c].b;
+          if (both) St::st2(dst[c] + idx, EnB[c].a, EnB[c].b, inv[c]);
+          else if (out0) St::st1(dst[c] + idx, EnB[c].a, inv[c]);
+          else St::st1(dst[c] + idx + 1, EnB[c].b, inv[c]);
         }
       }
       if (hB >= z0 && hB < z1) {
         const long long idx = x0 + (long long)y * pitch + (long long)hB * plane;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          if (both) st2(a.dst.f[3 + c] + idx, HnB[c].a, HnB[c].b);
-          else if (out0) a.dst.f[3 + c][idx] = HnB[c].a;
-          else a.dst.f[3 + c][idx + 1] = HnB[c].b;
+          if (both) St::st2(dst[3 + c] + idx, HnB[c].a, HnB[c].b, inv[3 + c]);
+          else if (out0) St::st1(dst[3 + c] + idx, HnB[c].a, inv[3 + c]);
+          else St::st1(dst[3 + c] + idx + 1, HnB[c].b, inv[3 + c]);
         }
       }
     }
   }
 
-  if (abort && tid == 0) {
-    for (int q = it + 1; q < niter && q < it + K::NS; ++q)
-      (void)mbar_wait_bounded(&bars[q % K::NS], (uint32_t)(q / K::NS) & 1u, kWaitLimit / 8);
+  if (abort) {
+    if (tid == 0) {
+      // Let copies that were already issued land before the shared memory is released.
+      for (int q = it + 1; q < niter && q < it + K::NS; ++q) {
+        const uint32_t uq = gbase + (uint32_t)q;
+        (void)mbar_wait_bounded(&bars[uq % K::NS], (uq / K::NS) & 1u, kWaitLimit / 8);
+      }
+    }
+    return false;
+  }
+  gbase += (uint32_t)niter;
+  return true;
+}
+
+template <typename S, int B, int TY>
+__device__ __forceinline__ Smem setup_smem(unsigned char* smem_raw, int* s_abort) {
+  using K = Tiled2<S, B, TY>;
+  unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  Smem sm{base, reinterpret_cast<uint64_t*>(base + K::OFF_BAR), s_abort};
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    *s_abort = 0;
+    for (int s = 0; s < K::NS; ++s) mbar_init(&sm.bars[s], 1);
+    fence_mbar_init();
+  }
+  return sm;
+}
+
+// One grid: one tile per CTA.  MINB > 1 caps registers so that MINB CTAs fit on an SM (more
+// warps to hide latency, at the cost of some spilled state); the autotuner decides.
+template <typename S, int B, int TY, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB)
+    fdtd_tiled2(const __grid_constant__ TiledArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ int s_abort;
+  const Smem sm = setup_smem<S, B, TY>(smem_raw, &s_abort);
+  uint32_t gbase = 0;
+  (void)march<S, B, TY>(a, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, sm, gbase, 0);
+}
+
+// A batch of independent grids: persistent CTAs pull (grid, tile) work items from a queue.
+template <typename S, int B, int TY>
+__global__ void __launch_bounds__(32 * TY, 1) fdtd_tiled2_batch(const BatchArgs b) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ int s_abort;
+  __shared__ int s_item;
+  const Smem sm = setup_smem<S, B, TY>(smem_raw, &s_abort);
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  uint32_t gbase = 0;
+  while (true) {
+    __syncthreads();  // every thread is done with the previous item (and s_item)
+    if (tid == 0) s_item = (int)atomicAdd(b.counter, 1u);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= b.nitems) break;
+    const int4 w = b.items[item];  // {grid, bx, by, bz}
+    const TiledArgs& a = b.grids[b.flip * b.ngrids + w.x];
+    if (!march<S, B, TY>(a, w.y, w.z, w.w, sm, gbase, b.t_offset)) break;
   }
 }
 
-template <int B, int TY, int MINB>
+template <typename S, int B, int TY, int MINB>
 cudaError_t launch_one2(const TiledArgs& a, dim3 grid, cudaStream_t st) {
-  using K = Tiled2<B, TY>;
-  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2<B, TY, MINB>,
+  using K = Tiled2<S, B, TY>;
+  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2<S, B, TY, MINB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
   if (e != cudaSuccess) return e;
-  fdtd_tiled2<B, TY, MINB><<<grid, dim3(32, TY), K::SMEM, st>>>(a);
+  fdtd_tiled2<S, B, TY, MINB><<<grid, dim3(32, TY), K::SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
-template <int TY>
+template <typename S, int B, int TY>
+cudaError_t launch_batch_one(const BatchArgs& b, int ctas, cudaStream_t st) {
+  using K = Tiled2<S, B, TY>;
+  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2_batch<S, B, TY>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
+  if (e != cudaSuccess) return e;
+  fdtd_tiled2_batch<S, B, TY><<<ctas, dim3(32, TY), K::SMEM, st>>>(b);
+  return cudaGetLastError();
+}
+
+template <typename S, int TY>
 cudaError_t launch_rows2(int blt, int min_blocks, const TiledArgs& a, dim3 grid,
                          cudaStream_t st) {
   if (min_blocks > 1) {
-    // register-capped variants: two CTAs of 16 rows or four of 8 rows per SM
-    if constexpr (TY == 16) {
-      if (blt == 2 && min_blocks == 2) return launch_one2<2, 16, 2>(a, grid, st);
+    // register-capped FP32 variants: two CTAs of 16 rows or four of 8 rows per SM
+    if constexpr (sizeof(S) == 4 && TY == 16) {
+      if (blt == 2 && min_blocks == 2) return launch_one2<S, 2, 16, 2>(a, grid, st);
     }
-    if constexpr (TY == 8) {
-      if (blt == 2 && min_blocks == 4) return launch_one2<2, 8, 4>(a, grid, st);
+    if constexpr (sizeof(S) == 4 && TY == 8) {
+      if (blt == 2 && min_blocks == 4) return launch_one2<S, 2, 8, 4>(a, grid, st);
     }
     return cudaErrorInvalidValue;
   }
   switch (blt) {
-    case 1: return launch_one2<1, TY, 1>(a, grid, st);
-    case 2: return launch_one2<2, TY, 1>(a, grid, st);
-    case 3: if constexpr (TY < 32) return launch_one2<3, TY, 1>(a, grid, st); break;
-    case 4: if constexpr (TY == 16) return launch_one2<4, TY, 1>(a, grid, st); break;
+    case 1: return launch_one2<S, 1, TY, 1>(a, grid, st);
+    case 2: return launch_one2<S, 2, TY, 1>(a, grid, st);
+    case 3: if constexpr (TY < 32) return launch_one2<S, 3, TY, 1>(a, grid, st); break;
+    case 4: if constexpr (TY == 16) return launch_one2<S, 4, TY, 1>(a, grid, st); break;
     default: break;
   }
   return cudaErrorInvalidValue;
 }
 
+template <typename S>
+cudaError_t launch_type2(const TiledConfig& c, const TiledArgs& a, dim3 grid, cudaStream_t st) {
+  switch (c.rows) {
+    case 8: return launch_rows2<S, 8>(c.blt, c.min_blocks, a, grid, st);
+    case 16: return launch_rows2<S, 16>(c.blt, c.min_blocks, a, grid, st);
+    case 32:
+      if constexpr (sizeof(S) == 4) return launch_rows2<S, 32>(c.blt, c.min_blocks, a, grid, st);
+      break;
+    default: break;
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename S>
+cudaError_t launch_batch_type(const TiledConfig& c, const BatchArgs& b, int ctas,
+                              cudaStream_t st) {
+  if (c.rows == 16) {
+    switch (c.blt) {
+      case 1: return launch_batch_one<S, 1, 16>(b, ctas, st);
+      case 2: return launch_batch_one<S, 2, 16>(b, ctas, st);
+      case 3: return launch_batch_one<S, 3, 16>(b, ctas, st);
+      case 4: return launch_batch_one<S, 4, 16>(b, ctas, st);
+      default: break;
+    }
+  } else if (c.rows == 8) {
+    switch (c.blt) {
+      case 1: return launch_batch_one<S, 1, 8>(b, ctas, st);
+      case 2: return launch_batch_one<S, 2, 8>(b, ctas, st);
+      case 3: return launch_batch_one<S, 3, 8>(b, ctas, st);
+      default: break;
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename S, int B, int TY>
+size_t smem_of() {
+  return Tiled2<S, B, TY>::SMEM;
+}
+
+template <typename S, int B, int TY>
+int occupancy_of() {
+  int n = 0;
+  cudaFuncSetAttribute(fdtd_tiled2_batch<S, B, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)Tiled2<S, B, TY>::SMEM);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fdtd_tiled2_batch<S, B, TY>, 32 * TY,
+                                                    Tiled2<S, B, TY>::SMEM) != cudaSuccess)
+    return 1;
+  return n > 0 ? n : 1;
+}
+
+template <typename S>
+int batch_occupancy_type(const TiledConfig& c) {
+  if (c.rows == 16) {
+    switch (c.blt) {
+      case 1: return occupancy_of<S, 1, 16>();
+      case 2: return occupancy_of<S, 2, 16>();
+      case 3: return occupancy_of<S, 3, 16>();
+      case 4: return occupancy_of<S, 4, 16>();
+    }
+  } else if (c.rows == 8) {
+    switch (c.blt) {
+      case 1: return occupancy_of<S, 1, 8>();
+      case 2: return occupancy_of<S, 2, 8>();
+      case 3: return occupancy_of<S, 3, 8>();
+    }
+  }
+  return 1;
+}
+
 }  // namespace
 
 bool tiled2_config_supported(const TiledConfig& c) {
+  if (c.esz != 4 && c.esz != 2) return false;
   if (c.rows != 8 && c.rows != 16 && c.rows != 32) return false;
+  if (c.rows == 32 && c.esz != 4) return false;
   if (c.blt < 1 || c.blt > 4) return false;
   if (c.rows == 8 && c.blt > 3) return false;
   if (c.rows == 32 && c.blt > 2) return false;  // 1024 threads: the pair state spills
-  if (c.min_blocks > 1 && !(c.blt == 2 && ((c.rows == 16 && c.min_blocks == 2) ||
-                                           (c.rows == 8 && c.min_blocks == 4))))
+  if (c.min_blocks > 1 && !(c.esz == 4 && c.blt == 2 &&
+                            ((c.rows == 16 && c.min_blocks == 2) ||
+                             (c.rows == 8 && c.min_blocks == 4))))
     return false;
   return c.z_chunks >= 1;
 }
 
+bool tiled2_batch_supported(const TiledConfig& c) {
+  if (c.esz != 4 && c.esz != 2) return false;
+  if (c.rows == 16) return c.blt >= 1 && c.blt <= 4;
+  if (c.rows == 8) return c.blt >= 1 && c.blt <= 3;
+  return false;
+}
+
 dim3 tiled2_grid(const TiledConfig& c, const Grid& g) {
-  const int sx = tiled2_sx(c.blt), sy = tiled_sy(c.blt, c.rows);
-  const int first = tiled_xbase(c.blt) + c.blt;
+  const int sx = tiled2_sx(c.blt, c.esz), sy = tiled_sy(c.blt, c.rows);
+  const int first = tiled2_xbase(c.blt, c.esz) + c.blt;
   const int ntx = (g.nx - first + sx - 1) / sx;
   const int nty = (g.ny + sy - 1) / sy;
   const int zlen = (g.nz + c.z_chunks - 1) / c.z_chunks;
@@ -402,14 +620,53 @@ dim3 tiled2_grid(const TiledConfig& c, const Grid& g) {
   return dim3(ntx, nty, nzc);
 }
 
+size_t tiled2_batch_smem(const TiledConfig& c) {
+  const bool h = c.esz == 2;
+  if (c.rows == 16) {
+    switch (c.blt) {
+      case 1: return h ? smem_of<__half, 1, 16>() : smem_of<float, 1, 16>();
+      case 2: return h ? smem_of<__half, 2, 16>() : smem_of<float, 2, 16>();
+      case 3: return h ? smem_of<__half, 3, 16>() : smem_of<float, 3, 16>();
+      case 4: return h ? smem_of<__half, 4, 16>() : smem_of<float, 4, 16>();
+    }
+  } else if (c.rows == 8) {
+    switch (c.blt) {
+      case 1: return h ? smem_of<__half, 1, 8>() : smem_of<float, 1, 8>();
+      case 2: return h ? smem_of<__half, 2, 8>() : smem_of<float, 2, 8>();
+      case 3: return h ? smem_of<__half, 3, 8>() : smem_of<float, 3, 8>();
+    }
+  }
+  return 0;
+}
+
+int tiled2_batch_ctas_per_sm(const TiledConfig& c) {
+  switch (c.storage) {
+    case 0: return batch_occupancy_type<float>(c);
+    case 1: return batch_occupancy_type<__half>(c);
+    case 2: return batch_occupancy_type<__nv_bfloat16>(c);
+  }
+  return 1;
+}
+
 cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& a, const Grid& g,
                           cudaStream_t st) {
   if (!tiled2_config_supported(c)) return cudaErrorInvalidValue;
   const dim3 grid = tiled2_grid(c, g);
-  switch (c.rows) {
-    case 8: return launch_rows2<8>(c.blt, c.min_blocks, a, grid, st);
-    case 16: return launch_rows2<16>(c.blt, c.min_blocks, a, grid, st);
-    case 32: return launch_rows2<32>(c.blt, c.min_blocks, a, grid, st);
+  switch (c.storage) {
+    case 0: return launch_type2<float>(c, a, grid, st);
+    case 1: return launch_type2<__half>(c, a, grid, st);
+    case 2: return launch_type2<__nv_bfloat16>(c, a, grid, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_tiled2_batch(const TiledConfig& c, const BatchArgs& b, int ctas,
+                                cudaStream_t st) {
+  if (!tiled2_batch_supported(c)) return cudaErrorInvalidValue;
+  switch (c.storage) {
+    case 0: return launch_batch_type<float>(c, b, ctas, st);
+    case 1: return launch_batch_type<__half>(c, b, ctas, st);
+    case 2: return launch_batch_type<__nv_bfloat16>(c, b, ctas, st);
     default: return cudaErrorInvalidValue;
   }
 }

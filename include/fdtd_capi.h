@@ -68,12 +68,15 @@ typedef enum fdtd_kernel {
   FDTD_KERNEL_TILED_W64 = 4   /* tiled, an x-pair of cells per thread (64-wide warp rows) */
 } fdtd_kernel;
 
-/* Field storage in HBM.  Arithmetic is FP32 in every case; F16/BF16 store each component
- * with a per-component scale (value = stored * scale). */
+/* Field storage in HBM.  F32/F16/BF16 update in FP32 arithmetic; F16/BF16 store each
+ * component with a per-component power-of-two scale (value = stored * scale) and run the tiled
+ * x-pair kernel only.  F64 stores and updates in FP64 with the naive kernel: the error
+ * reference for reduced-precision runs (coefficients and waveforms widened from FP32). */
 typedef enum fdtd_storage {
   FDTD_STORE_F32 = 0,
   FDTD_STORE_F16 = 1,
-  FDTD_STORE_BF16 = 2
+  FDTD_STORE_BF16 = 2,
+  FDTD_STORE_F64 = 3
 } fdtd_storage;
 
 typedef struct fdtd_desc {
@@ -150,8 +153,11 @@ fdtd_status fdtd_get_dft(fdtd_handle* h, int32_t monitor_id, double* re, double*
 fdtd_status fdtd_get_field_device(fdtd_handle* h, int32_t component, float* dev_out,
                                   void* stream);
 
-/* Per-component storage scale for F16/BF16 storage (ignored for F32); default 1. */
+/* Per-component storage scale for F16/BF16 storage (ignored otherwise); default 1.  Each scale
+ * is rounded to the nearest power of two, so scaling never rounds. */
 fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6);
+/* Field transfer into FP64 host memory (any storage; exact for F64 storage). */
+fdtd_status fdtd_get_field_f64(fdtd_handle* h, int32_t component, double* host_out);
 
 /* Kernel configuration actually used by the last fdtd_step: out = {kernel, blt, tile_rows,
  * z_chunks, launches in the last fdtd_step, min_blocks}; kernel is FDTD_KERNEL_NAIVE,
@@ -178,6 +184,26 @@ fdtd_status fdtd_build_material_map_noalloc(const float* const* coef12_dev, int6
                                             int64_t ny, int64_t nz, uint16_t* mat_dev,
                                             float* table_dev, int32_t max_materials,
                                             int32_t* nmat_out, void* stream);
+
+/* ---------------------------------------------------------------- batches
+ * Many independent simulations advanced together.  The reference runs one grid per call;
+ * here a batch groups existing handles (same device and storage, coefficients compressed to a
+ * material map) and fdtd_batch_step advances all of them with one persistent launch of the
+ * tiled x-pair kernel per BLT steps: CTAs pull (simulation, tile) work items, longest first,
+ * from an atomic queue, so grids of uneven size share the GPU without per-grid launches. */
+typedef struct fdtd_batch fdtd_batch;
+
+fdtd_status fdtd_batch_create(fdtd_handle* const* sims, int32_t n, fdtd_batch** out);
+fdtd_status fdtd_batch_destroy(fdtd_batch* b);
+/* Advances every simulation of the batch by T steps from its own state (step counter, fields,
+ * sources, monitors).  use_graph != 0: the launch sequence is captured in a CUDA graph the
+ * first time and replayed while (T, each simulation's step counter and field set) repeat.
+ * stream: a cudaStream_t or NULL for the batch's own stream. */
+fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* stream);
+/* out = {blt, tile_rows, persistent CTAs, work items per launch, launches in the last step,
+ * 1 if the last step replayed a graph}. */
+fdtd_status fdtd_batch_get_config(const fdtd_batch* b, int32_t* out6);
+const char* fdtd_batch_last_error(const fdtd_batch* b);
 
 #ifdef __cplusplus
 }
