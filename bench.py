@@ -346,6 +346,200 @@ def run_ours(args):
     return 0
 
 
+# ------------------------------------------------------------------ other configurations
+
+
+def _spectral_error(a, b):
+    """Relative L2 error of complex spectra a = (re, im) lists against b."""
+    num = sum(np.sum((ar - br) ** 2 + (ai - bi) ** 2) for (ar, ai), (br, bi) in zip(a, b))
+    den = sum(np.sum(br ** 2 + bi ** 2) for (br, bi) in b)
+    return float(np.sqrt(num / den))
+
+
+def _field_error(F, R):
+    num = sum(np.sum((f.astype(np.float64) - r) ** 2) for f, r in zip(F, R))
+    den = sum(np.sum(r ** 2) for r in R)
+    return float(np.sqrt(num / den))
+
+
+def _timed(fn, reps=1):
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fn()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) / reps
+
+
+def fp16_scales(probe, ncell, T, every=20, headroom=16384.0):
+    """Power-of-two FP16 storage scales from the field peaks of an FP32 run: the largest |value|
+    of the E components (and, separately, of the H components) seen in snapshots every `every`
+    steps maps to at most `headroom` (4x below the FP16 maximum).  One scale per field rather
+    than per component: a component that is zero by symmetry in the probe (Hz of a Jz dipole)
+    can grow later by scattering.  Closes `probe`."""
+    import torch
+    peaks = [0.0] * 6
+    buf = torch.empty(ncell, dtype=torch.float32, device="cuda")
+    for _ in range(0, T, every):
+        probe.step(every)
+        for c in range(6):
+            probe.get_field_device(c, buf.data_ptr())
+            torch.cuda.synchronize()
+            peaks[c] = max(peaks[c], float(buf.abs().max()))
+    probe.close()
+    e, h = max(peaks[:3]), max(peaks[3:])
+    se = float(2.0 ** np.ceil(np.log2(max(e, 1e-30) / headroom)))
+    sh = float(2.0 ** np.ceil(np.log2(max(h, 1e-30) / headroom)))
+    return [se, se, se, sh, sh, sh]
+
+
+def run_mixed(args):
+    """Mixed-precision FDTD: 512x512x384 grid, 200 seeded dielectric spheres, Gaussian Jz at the
+    centre, FP64 running DFT of Ez at 16 frequencies on the planes z=96 and z=288, 2000 steps.
+    FP32, BF16 and FP16 field storage against an FP64 run of the same grid."""
+    import torch
+    import gdiamond_b200 as gd
+    from gdiamond_b200 import workloads as W
+    shape = tuple(int(v) for v in args.grid.split(",")) if args.grid != "256,256,256" else (512, 512, 384)
+    T = args.timesteps if args.timesteps != T_STEPS else 2000
+    nx, ny, nz = shape
+    eps = W.spheres_eps(shape, n_spheres=200, r_range=(4, 24), eps_range=(1.0, 12.0), seed=0)
+    wave = W.gaussian_wave(T)
+    freqs = W.source_band(16)
+    planes = (nz * 96 // 384, nz * 288 // 384)
+    src = [dict(component="Jz", wave=wave, i=nx // 2, j=ny // 2, k=nz // 2)]
+    ncell = nx * ny * nz
+
+    def make(storage, scales=None):
+        sim = gd.Simulation(nx, ny, nz, storage=storage)
+        if scales is not None:
+            sim.set_storage_scale(scales)
+        sim.set_permittivity(eps)
+        sim.set_sources(src)
+        for k in planes:
+            sim.add_dft_monitor("Ez", k, freqs, scale=1.0)
+        return sim
+
+    res = {}
+    ref = make("f64")
+    t64 = _timed(lambda: ref.step(T) or ref.sync())
+    R = [ref.get_field_f64(c) for c in range(6)]
+    D64 = [ref.get_dft(m) for m in range(2)]
+    nmat = ref.material_count()
+    ref.close()
+    res["f64"] = {"gcells": ncell * T / t64 / 1e9, "seconds": t64}
+    f16_scales = fp16_scales(make("f32"), ncell, min(T, 400))
+    for storage, scales in (("f32", None), ("bf16", None), ("f16", f16_scales)):
+        sim = make(storage, scales)
+        sim.step(2 * 4)  # autotune + warm-up outside the timed run
+        sim.reset()
+        dt_ = _timed(lambda: sim.step(T) or sim.sync())
+        F = [sim.get_field(c) for c in range(6)]
+        D = [sim.get_dft(m) for m in range(2)]
+        cfg = sim.config()
+        sim.close()
+        res[storage] = {"gcells": ncell * T / dt_ / 1e9, "seconds": dt_,
+                        "spectral_rel_err_vs_f64": _spectral_error(D, D64),
+                        "field_rel_l2_vs_f64": _field_error(F, R),
+                        "kernel": cfg, "scales": scales}
+    line = {"metric": "Gcell-updates/s and relative error vs FP64", "workload":
+            f"fdtd3d_{nx}x{ny}x{nz}_200spheres_gaussJz_T{T}_dft16x2planes",
+            "materials": nmat, "results": res, "data": "synthetic (seeded spheres)"}
+    print(json.dumps(line))
+    return 0
+
+
+def run_batched(args):
+    """64 independent uneven simulations (sides from {64,96,128,160,192} per axis, seeded), one
+    dielectric slab each, Gaussian Jz at a random interior point, 32-frequency DFT of Ez on one
+    plane each, 2000 steps.  Spectra/s of the batched persistent solver (16-bit storage,
+    CUDA graph) against the plain FP32 solver run simulation by simulation; spectral error of
+    both against FP64 runs."""
+    import gdiamond_b200 as gd
+    from gdiamond_b200 import workloads as W
+    n_sims = args.sims
+    T = args.timesteps if args.timesteps != T_STEPS else 2000
+    rng = np.random.default_rng(4)
+    sides = (64, 96, 128, 160, 192)
+    specs = []
+    for _ in range(n_sims):
+        shape = tuple(int(rng.choice(sides)) for _ in range(3))
+        eps = W.slab_eps(shape, rng)
+        pos = tuple(int(rng.integers(12, s - 12)) for s in shape)
+        specs.append((shape, eps, pos))
+    freqs = W.source_band(32)
+    wave = W.gaussian_wave(T)
+    total_cells = sum(int(np.prod(s[0])) for s in specs)
+
+    def make(spec, storage, scales=None):
+        shape, eps, pos = spec
+        sim = gd.Simulation(*shape, storage=storage)
+        if scales is not None:
+            sim.set_storage_scale(scales)
+        sim.set_permittivity(eps)
+        sim.set_sources([dict(component="Jz", wave=wave, i=pos[0], j=pos[1], k=pos[2])])
+        sim.add_dft_monitor("Ez", (3 * shape[2]) // 4, freqs, scale=1.0)
+        return sim
+
+    def run_each(storage):
+        sims = [make(sp, storage) for sp in specs]
+        for s in sims:  # autotune each shape outside the timed region
+            s.step(4)
+            s.reset()
+        dt_ = _timed(lambda: [s.step(T) for s in sims] and [s.sync() for s in sims])
+        D = [s.get_dft(0) for s in sims]
+        for s in sims:
+            s.close()
+        return dt_, D
+
+    t64, D64 = run_each("f64")
+    t32, D32 = run_each("f32")
+    out = {"plain_f32_sim_by_sim": {"seconds": t32, "spectra_per_s": n_sims / t32,
+                                    "gcells": total_cells * T / t32 / 1e9,
+                                    "spectral_rel_err_vs_f64": float(np.mean(
+                                        [_spectral_error([a], [b]) for a, b in zip(D32, D64)]))},
+           "f64_sim_by_sim": {"seconds": t64, "spectra_per_s": n_sims / t64}}
+    # FP16 scales valid for every simulation: the fields peak at the source during the pulse
+    # and are largest in vacuum (a dielectric lowers Cb), so probe a vacuum copy of the most
+    # confined simulation with its source.
+    small = min(range(n_sims), key=lambda i: min(specs[i][0]))
+    shape0, _, pos0 = specs[small]
+    f16 = fp16_scales(make((shape0, np.ones(int(np.prod(shape0)), np.float32), pos0), "f32"),
+                      int(np.prod(shape0)), min(T, 300))
+    for storage in ("bf16", "f16"):
+        scales = f16 if storage == "f16" else None
+        sims = [make(sp, storage, scales) for sp in specs]
+        batch = gd.Batch(sims)
+        batch.step(4)  # batch autotune outside the timed region
+        for s in sims:
+            s.reset()
+        batch.step(T)  # captures the graph
+        for s in sims:
+            s.reset()
+
+        def one():
+            batch.step(T)
+            for s in sims:
+                s.sync()
+        dt_ = _timed(one)
+        D = [s.get_dft(0) for s in sims]
+        cfg = batch.config()
+        errs = [_spectral_error([a], [b]) for a, b in zip(D, D64)]
+        batch.close()
+        for s in sims:
+            s.close()
+        out[f"batched_{storage}_graph"] = {
+            "seconds": dt_, "spectra_per_s": n_sims / dt_, "gcells": total_cells * T / dt_ / 1e9,
+            "speedup_vs_plain_f32": t32 / dt_, "spectral_rel_err_vs_f64_mean": float(np.mean(errs)),
+            "spectral_rel_err_vs_f64_max": float(np.max(errs)), "config": cfg}
+    line = {"metric": "spectra/s (batched vs plain) at stated spectral error vs FP64",
+            "workload": f"{n_sims} uneven sims, sides from {sides}, slab each, T={T}, 32-freq DFT",
+            "total_cells": total_cells, "results": out, "data": "synthetic (seeded)"}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -362,9 +556,17 @@ def main():
     ap.add_argument("--rows", type=int, default=0, help="force tile rows")
     ap.add_argument("--zchunks", type=int, default=0, help="force z-chunks")
     ap.add_argument("--min-blocks", type=int, default=0, help="force the register cap")
+    ap.add_argument("--workload", default="plain", choices=["plain", "mixed", "batched"],
+                    help="plain: the benchmark line; mixed / batched: the precision and "
+                         "batching configurations (separate JSON lines)")
+    ap.add_argument("--sims", type=int, default=64, help="batched workload: simulations")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "mixed":
+        return run_mixed(args)
+    if args.workload == "batched":
+        return run_batched(args)
     return run_ours(args)
 
 

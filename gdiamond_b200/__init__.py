@@ -35,7 +35,7 @@ EXPORTS = (
     "fdtd_get_field_device", "fdtd_set_storage_scale", "fdtd_get_config",
     "fdtd_build_material_map_noalloc", "fdtd_get_field_f64",
     "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_step", "fdtd_batch_get_config",
-    "fdtd_batch_last_error",
+    "fdtd_batch_last_error", "fdtd_set_permittivity", "fdtd_get_coefficients",
 )
 
 
@@ -96,6 +96,8 @@ def library():
             "fdtd_batch_step": ([V, C.c_int64, C.c_int32, V], C.c_int),
             "fdtd_batch_get_config": ([V, P(C.c_int32)], C.c_int),
             "fdtd_batch_last_error": ([V], C.c_char_p),
+            "fdtd_set_permittivity": ([V, P(C.c_float), C.c_int32, C.c_float, C.c_float], C.c_int),
+            "fdtd_get_coefficients": ([V, P(P(C.c_float))], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -174,6 +176,26 @@ class Simulation:
                 raise ValueError("coefficient array size mismatch")
         arr = (C.POINTER(C.c_float) * 12)(*[_fp(c) for c in cs])
         self._check(self._L.fdtd_set_coefficients(self._h, arr))
+
+    def set_permittivity(self, eps_re=None, t_pml=10, dt=np.float32(0.05),
+                         omega0=np.float32(2) * np.float32(3.14159265359)):
+        """gDiamond's constructor coefficients (graded pseudo-PML) for a per-cell relative
+        permittivity (None = vacuum), computed on the GPU."""
+        e = None
+        if eps_re is not None:
+            e = np.ascontiguousarray(eps_re, np.float32).reshape(-1)
+            if e.size != self.ncells:
+                raise ValueError("permittivity size mismatch")
+            self._keep_eps = e
+        self._check(self._L.fdtd_set_permittivity(self._h, None if e is None else _fp(e),
+                                                   int(t_pml), float(np.float32(dt)),
+                                                   float(np.float32(omega0))))
+
+    def get_coefficients(self):
+        out = [np.empty(self.ncells, np.float32) for _ in range(12)]
+        arr = (C.POINTER(C.c_float) * 12)(*[_fp(c) for c in out])
+        self._check(self._L.fdtd_get_coefficients(self._h, arr))
+        return out
 
     def material_count(self):
         n = C.c_int32()

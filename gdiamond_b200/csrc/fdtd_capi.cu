@@ -405,17 +405,45 @@ void free_all(fdtd_handle* h) {
   if (h->stream) cudaStreamDestroy(h->stream);
 }
 
-fdtd_status upload_coefficients(fdtd_handle* h, const float* const* src, cudaMemcpyKind kind) {
+fdtd_status alloc_coef_staging(fdtd_handle* h) {
   const size_t bytes = h->cells * sizeof(float);
-  for (int a = 0; a < 12; ++a) {
-    if (!src[a]) return fail(h, FDTD_ERR_INVALID_ARG, "coefficient array %d is NULL", a);
+  for (int a = 0; a < 12; ++a)
     if (!h->coef[a]) {
       CUDA_TRY(h, cudaMalloc(&h->coef[a], bytes));
       CUDA_TRY(h, cudaMemsetAsync(h->coef[a], 0, bytes, h->stream));
     }
+  return FDTD_OK;
+}
+
+fdtd_status compress_coefficients(fdtd_handle* h);
+
+fdtd_status upload_coefficients(fdtd_handle* h, const float* const* src, cudaMemcpyKind kind) {
+  for (int a = 0; a < 12; ++a)
+    if (!src[a]) return fail(h, FDTD_ERR_INVALID_ARG, "coefficient array %d is NULL", a);
+  fdtd_status s = alloc_coef_staging(h);
+  if (s != FDTD_OK) return s;
+  for (int a = 0; a < 12; ++a)
     CUDA_TRY(h, cudaMemcpy2DAsync(h->coef[a], (size_t)h->g.pitch * 4, src[a], (size_t)h->g.nx * 4,
                                   (size_t)h->g.nx * 4, (size_t)h->g.ny * h->g.nz, kind, h->stream));
+  return compress_coefficients(h);
+}
+
+// One axis of graded stretch factors (gDiamond/utils.h:585-619), evaluated on the host with the
+// C library's pow exactly as the reference does.
+std::vector<float2> stretch_profile(int n, int t_pml, float sigma_max, float omega0) {
+  std::vector<float2> out(n);
+  for (int i = 0; i < n; ++i) {
+    float dist = 0;
+    if (i < t_pml) dist = (float)(1.0 - (double)((float)i / (float)t_pml));
+    if (i + t_pml >= n) dist = (float)(1.0 - (double)((float)(n - i - 1) / (float)t_pml));
+    const double d3 = std::pow((double)dist, 3.0);
+    out[i] = make_float2((float)(1.0 + (double)2.0f * d3),
+                         (float)((double)sigma_max * d3 / (double)(omega0 * 1.0f)));
   }
+  return out;
+}
+
+fdtd_status compress_coefficients(fdtd_handle* h) {
   if (!h->mat) {
     CUDA_TRY(h, cudaMalloc(&h->mat, h->cells * sizeof(uint16_t)));
     CUDA_TRY(h, cudaMemsetAsync(h->mat, 0, h->cells * sizeof(uint16_t), h->stream));
@@ -545,6 +573,57 @@ fdtd_status fdtd_set_coefficients_device(fdtd_handle* h, const float* const* coe
   if (!h || !coef12_dev) return FDTD_ERR_INVALID_ARG;
   DeviceGuard dg(h->desc.device);
   return upload_coefficients(h, coef12_dev, cudaMemcpyDeviceToDevice);
+}
+
+fdtd_status fdtd_set_permittivity(fdtd_handle* h, const float* eps_re, int32_t t_pml, float dt,
+                                  float omega0) {
+  if (!h || t_pml < 1 || !(dt > 0) || !(omega0 > 0)) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  fdtd_status s = alloc_coef_staging(h);
+  if (s != FDTD_OK) return s;
+  const float dx = h->desc.dx;
+  const float denom = 2 * 1.0f * (float)t_pml * dx;
+  const float sigma_max = (float)((double)(-4) * std::log(1e-5) / (double)denom);
+  std::vector<float2> prof[3] = {stretch_profile(h->g.nx, t_pml, sigma_max, omega0),
+                                 stretch_profile(h->g.ny, t_pml, sigma_max, omega0),
+                                 stretch_profile(h->g.nz, t_pml, sigma_max, omega0)};
+  const size_t n = (size_t)h->g.nx * h->g.ny * h->g.nz;
+  float2* d_prof = nullptr;
+  float* d_eps = nullptr;
+  const size_t np = prof[0].size() + prof[1].size() + prof[2].size();
+  CUDA_TRY(h, cudaMalloc(&d_prof, np * sizeof(float2)));
+  CUDA_TRY(h, cudaMemcpyAsync(d_prof, prof[0].data(), prof[0].size() * 8, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(d_prof + prof[0].size(), prof[1].data(), prof[1].size() * 8,
+                              cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(d_prof + prof[0].size() + prof[1].size(), prof[2].data(),
+                              prof[2].size() * 8, cudaMemcpyHostToDevice, h->stream));
+  if (eps_re) {
+    CUDA_TRY(h, cudaMalloc(&d_eps, n * sizeof(float)));
+    CUDA_TRY(h, cudaMemcpyAsync(d_eps, eps_re, n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+  }
+  fdtd::Coef12Out out;
+  for (int a = 0; a < 12; ++a) out.c[a] = h->coef[a];
+  CUDA_TRY(h, fdtd::build_coefficients(h->g, d_eps, d_prof, d_prof + prof[0].size(),
+                                       d_prof + prof[0].size() + prof[1].size(), omega0, dt, dx,
+                                       out, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  cudaFree(d_prof);
+  cudaFree(d_eps);
+  return compress_coefficients(h);
+}
+
+fdtd_status fdtd_get_coefficients(fdtd_handle* h, float* const* out12) {
+  if (!h || !out12) return FDTD_ERR_INVALID_ARG;
+  if (!h->coef[0]) return fail(h, FDTD_ERR_INVALID_ARG, "coefficients are not set");
+  DeviceGuard dg(h->desc.device);
+  for (int a = 0; a < 12; ++a) {
+    if (!out12[a]) return FDTD_ERR_INVALID_ARG;
+    CUDA_TRY(h, cudaMemcpy2DAsync(out12[a], (size_t)h->g.nx * 4, h->coef[a], (size_t)h->g.pitch * 4,
+                                  (size_t)h->g.nx * 4, (size_t)h->g.ny * h->g.nz,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return FDTD_OK;
 }
 
 fdtd_status fdtd_material_count(const fdtd_handle* h, int32_t* nmat) {
@@ -853,6 +932,7 @@ struct fdtd_batch {
   cudaStream_t stream = nullptr;
   int storage = 0, esz = 4;
   fdtd::TiledConfig cfg{0, 0, 1, 64};
+  int zlen = 0;  // target z-chunk length of a work item (0: whole columns)
   bool cfg_ready = false;
   fdtd::TiledArgs* d_args = nullptr;  // [2][n]
   fdtd::TiledArgs* h_args = nullptr;  // pinned staging [2][n]
@@ -892,10 +972,13 @@ fdtd::TiledConfig batch_cfg(const fdtd_batch* b, int blt, int rows) {
   return c;
 }
 
-// Work items of one BLT value: every tile column of every simulation (one z-chunk: the whole
-// column is one item), longest z-march first so the queue's tail is short.
+// z-chunks of one simulation for a target chunk length (0: one chunk per column).
+int sim_chunks(const Grid& g, int zlen) { return zlen <= 0 ? 1 : std::max(1, (g.nz + zlen - 1) / zlen); }
+
+// Work items of one (BLT, rows, chunk length): every z-chunk of every tile column of every
+// simulation, longest z-march first so the queue's tail is short.
 fdtd_status batch_items(fdtd_batch* b, const fdtd::TiledConfig& c, std::pair<int4*, int>* out) {
-  const int key = c.blt * 100 + c.rows;
+  const int key = (b->zlen * 10 + c.blt) * 100 + c.rows;
   auto it = b->items.find(key);
   if (it != b->items.end()) {
     *out = it->second;
@@ -904,10 +987,14 @@ fdtd_status batch_items(fdtd_batch* b, const fdtd::TiledConfig& c, std::pair<int
   std::vector<std::pair<int, int4>> v;
   for (size_t i = 0; i < b->sims.size(); ++i) {
     const Grid& g = b->sims[i]->g;
-    const dim3 gd = fdtd::tiled2_grid(c, g);
-    for (unsigned by = 0; by < gd.y; ++by)
-      for (unsigned bx = 0; bx < gd.x; ++bx)
-        v.push_back({g.nz, make_int4((int)i, (int)bx, (int)by, 0)});
+    fdtd::TiledConfig ci = c;
+    ci.z_chunks = sim_chunks(g, b->zlen);
+    const dim3 gd = fdtd::tiled2_grid(ci, g);
+    const int len = (g.nz + ci.z_chunks - 1) / ci.z_chunks + 2 * c.blt;
+    for (unsigned bz = 0; bz < gd.z; ++bz)
+      for (unsigned by = 0; by < gd.y; ++by)
+        for (unsigned bx = 0; bx < gd.x; ++bx)
+          v.push_back({len, make_int4((int)i, (int)bx, (int)by, (int)bz)});
   }
   std::stable_sort(v.begin(), v.end(),
                    [](const std::pair<int, int4>& a, const std::pair<int, int4>& b2) {
@@ -937,7 +1024,7 @@ void batch_fill_args(fdtd_batch* b, const fdtd::TiledConfig& c, bool with_io) {
   for (size_t i = 0; i < n; ++i) {
     fdtd_handle* h = b->sims[i];
     fdtd::TiledConfig ci = c;
-    ci.z_chunks = 1;
+    ci.z_chunks = sim_chunks(h->g, b->zlen);
     for (int p = 0; p < 2; ++p)
       b->h_args[p * n + i] = make_tiled_args(h, ci, h->t, with_io, h->cur ^ p);
   }
@@ -991,9 +1078,11 @@ fdtd_status batch_autotune(fdtd_batch* b, cudaStream_t st) {
   BCUDA(b, cudaEventCreate(&e1));
   float best = 1e30f;
   fdtd::TiledConfig best_c = cands[0];
-  int best_ctas = nsm;
+  int best_ctas = nsm, best_zlen = 0;
   for (int pass = 0; pass < 2; ++pass)  // the first pass also brings the clocks up
-    for (const auto& c : cands) {
+    for (const auto& c : cands)
+    for (int zl : {0, 64, 32}) {
+      b->zlen = zl;
       if ((s = batch_maps(b, c.rows)) != FDTD_OK) return s;
       b->ctas = nsm * fdtd::tiled2_batch_ctas_per_sm(c);
       batch_fill_args(b, c, false);
@@ -1013,12 +1102,14 @@ fdtd_status batch_autotune(fdtd_batch* b, cudaStream_t st) {
         best = per_step;
         best_c = c;
         best_ctas = b->ctas;
+        best_zlen = zl;
       }
     }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   b->cfg = best_c;
   b->ctas = best_ctas;
+  b->zlen = best_zlen;
   b->cfg_ready = true;
   return FDTD_OK;
 }
@@ -1124,7 +1215,7 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
 
   b->last_graph = 0;
   if (use_graph) {
-    std::vector<long long> key = {T, c.blt, c.rows, b->ctas};
+    std::vector<long long> key = {T, c.blt, c.rows, b->ctas, b->zlen};
     for (fdtd_handle* h : b->sims) {
       key.push_back(h->t);
       key.push_back(h->cur);
@@ -1169,7 +1260,7 @@ fdtd_status fdtd_batch_get_config(const fdtd_batch* b, int32_t* out6) {
   out6[0] = b->cfg.blt;
   out6[1] = b->cfg.rows;
   out6[2] = b->ctas;
-  auto it = b->items.find(b->cfg.blt * 100 + b->cfg.rows);
+  auto it = b->items.find((b->zlen * 10 + b->cfg.blt) * 100 + b->cfg.rows);
   out6[3] = it == b->items.end() ? 0 : it->second.second;
   out6[4] = b->last_launches;
   out6[5] = b->last_graph;

@@ -101,6 +101,16 @@ dim3 tiled_grid(const TiledConfig& c, const Grid& g);
 cudaError_t launch_tiled(const TiledConfig& c, const TiledArgs& args, const Grid& g,
                          cudaStream_t st);
 
+// ---------------------------------------------------------------- coefficient builder
+struct Coef12Out {
+  float* c[12];  // pitched per-cell arrays Cax..Dbz
+};
+// gDiamond's coefficient formula per cell from a per-cell permittivity (eps_dev: unpitched
+// nx*ny*nz floats, or nullptr for vacuum) and per-axis complex stretch factors (re, im).
+cudaError_t build_coefficients(const Grid& g, const float* eps_dev, const float2* sx,
+                               const float2* sy, const float2* sz, float omega0, float dt,
+                               float dx, const Coef12Out& out, cudaStream_t st);
+
 // ---------------------------------------------------------------- material dedup
 struct DedupResult {
   int nmat;        // distinct 12-tuples (valid when ok)

@@ -118,6 +118,17 @@ fdtd_status fdtd_set_coefficients(fdtd_handle* h, const float* const* coef12);
 fdtd_status fdtd_set_coefficients_device(fdtd_handle* h, const float* const* coef12_dev);
 /* Number of distinct materials found (0 when the per-cell arrays are in use). */
 fdtd_status fdtd_material_count(const fdtd_handle* h, int32_t* nmat);
+/* The coefficients of gDiamond's constructor (gDiamond/gdiamond.hpp:20-73 calling
+ * set_FDTD_matrices_3D_structure, gDiamond/utils.h:542-690) for a per-cell relative
+ * permittivity, computed on the GPU with the reference's arithmetic (bit-identical arrays):
+ * a graded pseudo-PML of t_pml cells on every face, time step dt, source omega omega0 (the
+ * reference's defaults are t_pml = 10, dt = 0.05, omega0 = 2*pi), spacing = desc.dx.
+ * eps_re: host array of Nx*Ny*Nz floats, or NULL for vacuum.  Then compressed as in
+ * fdtd_set_coefficients. */
+fdtd_status fdtd_set_permittivity(fdtd_handle* h, const float* eps_re, int32_t t_pml, float dt,
+                                  float omega0);
+/* Copies the per-cell coefficients last set (12 host arrays of Nx*Ny*Nz floats). */
+fdtd_status fdtd_get_coefficients(fdtd_handle* h, float* const* coef12_out);
 
 /* Replaces the source list.  waveforms = nsrc rows of T_wave FP32 samples; sample t drives
  * step t of the run (replaces the per-step 4-byte cudaMemcpy of the source value,
@@ -200,8 +211,8 @@ fdtd_status fdtd_batch_destroy(fdtd_batch* b);
  * first time and replayed while (T, each simulation's step counter and field set) repeat.
  * stream: a cudaStream_t or NULL for the batch's own stream. */
 fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* stream);
-/* out = {blt, tile_rows, persistent CTAs, work items per launch, launches in the last step,
- * 1 if the last step replayed a graph}. */
+/* out = {blt, tile_rows, persistent CTAs, work items per launch (tile columns x z-chunks),
+ * launches in the last step, 1 if the last step replayed a graph}. */
 fdtd_status fdtd_batch_get_config(const fdtd_batch* b, int32_t* out6);
 const char* fdtd_batch_last_error(const fdtd_batch* b);
 

@@ -267,3 +267,21 @@ def test_invalid_arguments_return_status():
         sim.add_dft_monitor("Ez", 10, [1.0])
     assert e.value.status == 4
     sim.close()
+
+
+@pytest.mark.parametrize("shape", [(37, 29, 23), (64, 48, 40)])
+def test_gpu_coefficient_builder_matches_reference_formula(shape):
+    """fdtd_set_permittivity computes gDiamond's constructor coefficients on the GPU."""
+    eps = W.spheres_eps(shape, n_spheres=8, r_range=(2, 8), seed=2)
+    for e in (None, eps):
+        ref = oracle.coefficients(shape, eps_re=e)  # pinned to the reference constructor
+        sim = gd.Simulation(*shape)
+        sim.set_permittivity(e)
+        got = sim.get_coefficients()
+        for a in range(12):
+            assert np.array_equal(got[a].view(np.uint32), ref[a].view(np.uint32)), oracle.COEFFS[a]
+        sim2 = gd.Simulation(*shape)
+        sim2.set_coefficients(ref)
+        assert sim.material_count() == sim2.material_count() > 1
+        sim.close()
+        sim2.close()
