@@ -372,12 +372,14 @@ def _timed(fn, reps=1):
     return (time.perf_counter() - t0) / reps
 
 
-def fp16_scales(probe, ncell, T, every=20, headroom=16384.0):
+def fp16_scales(probe, ncell, T, every=1, headroom=2048.0):
     """Power-of-two FP16 storage scales from the field peaks of an FP32 run: the largest |value|
-    of the E components (and, separately, of the H components) seen in snapshots every `every`
-    steps maps to at most `headroom` (4x below the FP16 maximum).  One scale per field rather
-    than per component: a component that is zero by symmetry in the probe (Hz of a Jz dipole)
-    can grow later by scattering.  Closes `probe`."""
+    of the E components (and, separately, of the H components) seen after every step of the
+    first T steps maps to at most `headroom` (32x below the FP16 maximum, since the field at
+    a point source swings between samples and later scattering can focus it; FP16's
+    2^30 range of normal numbers leaves the decayed late-time fields far above its subnormals
+    either way).  One scale per field rather than per component: a component that is zero by
+    symmetry in the probe (Hz of a Jz dipole) can grow later by scattering.  Closes `probe`."""
     import torch
     peaks = [0.0] * 6
     buf = torch.empty(ncell, dtype=torch.float32, device="cuda")

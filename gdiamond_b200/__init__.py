@@ -36,6 +36,9 @@ EXPORTS = (
     "fdtd_build_material_map_noalloc", "fdtd_get_field_f64",
     "fdtd_batch_create", "fdtd_batch_destroy", "fdtd_batch_step", "fdtd_batch_get_config",
     "fdtd_batch_last_error", "fdtd_set_permittivity", "fdtd_get_coefficients",
+    "fdtd_mlp_create", "fdtd_mlp_destroy", "fdtd_mlp_last_error", "fdtd_mlp_layout",
+    "fdtd_mlp_get_params", "fdtd_mlp_set_params", "fdtd_mlp_set_data", "fdtd_mlp_grad",
+    "fdtd_mlp_train", "fdtd_mlp_predict", "fdtd_mlp_predict_device", "fdtd_get_dft_device",
 )
 
 
@@ -91,6 +94,7 @@ def library():
             "fdtd_set_storage_scale": ([V, P(C.c_float)], C.c_int),
             "fdtd_get_config": ([V, P(C.c_int32)], C.c_int),
             "fdtd_get_field_f64": ([V, C.c_int32, P(C.c_double)], C.c_int),
+            "fdtd_get_dft_device": ([V, C.c_int32, V, V, V], C.c_int),
             "fdtd_batch_create": ([P(V), C.c_int32, P(V)], C.c_int),
             "fdtd_batch_destroy": ([V], C.c_int),
             "fdtd_batch_step": ([V, C.c_int64, C.c_int32, V], C.c_int),
@@ -98,6 +102,21 @@ def library():
             "fdtd_batch_last_error": ([V], C.c_char_p),
             "fdtd_set_permittivity": ([V, P(C.c_float), C.c_int32, C.c_float, C.c_float], C.c_int),
             "fdtd_get_coefficients": ([V, P(P(C.c_float))], C.c_int),
+            "fdtd_mlp_create": ([P(C.c_int32), C.c_int32, C.c_int32, C.c_uint64, C.c_int32,
+                                 P(V)], C.c_int),
+            "fdtd_mlp_destroy": ([V], C.c_int),
+            "fdtd_mlp_last_error": ([V], C.c_char_p),
+            "fdtd_mlp_layout": ([V, P(C.c_int64), P(C.c_int64), P(C.c_int64)], C.c_int),
+            "fdtd_mlp_get_params": ([V, P(C.c_float)], C.c_int),
+            "fdtd_mlp_set_params": ([V, P(C.c_float)], C.c_int),
+            "fdtd_mlp_set_data": ([V, P(C.c_float), P(C.c_float), C.c_int64], C.c_int),
+            "fdtd_mlp_grad": ([V, P(C.c_float), P(C.c_float), C.c_int64, P(C.c_float),
+                               P(C.c_float)], C.c_int),
+            "fdtd_mlp_train": ([V, C.c_int32, C.c_int32, C.c_float, C.c_uint64, P(C.c_float)],
+                               C.c_int),
+            "fdtd_mlp_predict": ([V, P(C.c_float), C.c_int64, P(C.c_float), P(C.c_float),
+                                  P(C.c_float)], C.c_int),
+            "fdtd_mlp_predict_device": ([V, V, C.c_int64, V, V, V], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -301,6 +320,14 @@ class Simulation:
                                           _fp(im, C.c_double)))
         return re, im
 
+    def get_dft_device(self, monitor_id, re_ptr, im_ptr, stream=None):
+        """Copy a monitor's running sums into device arrays (float64 [nf][ny][nx] pointers)."""
+        s = None
+        if stream is not None:
+            s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        self._check(self._L.fdtd_get_dft_device(self._h, int(monitor_id), C.c_void_p(re_ptr),
+                                                 C.c_void_p(im_ptr), s))
+
 
 class Batch:
     """Independent simulations advanced together by persistent launches (fdtd_batch_*).
@@ -339,6 +366,109 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             self._L.fdtd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MLP:
+    """An ensemble of MLPs trained and evaluated on the GPU (fdtd_mlp_*).
+
+    dims = (inputs, hidden..., outputs); GELU between layers; BF16 tensor-core GEMMs with FP32
+    accumulation and FP32 master weights; Adam.  Parameters of all members as one array
+    [members][n_params]; ``layout()`` gives each layer's weight and bias offsets.
+    """
+
+    def __init__(self, dims, members=4, seed=0, device=0):
+        self.dims = tuple(int(d) for d in dims)
+        self.members = int(members)
+        self._L = library()
+        d = (C.c_int32 * len(self.dims))(*self.dims)
+        h = C.c_void_p()
+        st = self._L.fdtd_mlp_create(d, len(self.dims), self.members, int(seed), int(device),
+                                     C.byref(h))
+        if st != 0:
+            raise FdtdError(st, "fdtd_mlp_create failed")
+        self._h = h
+        n = C.c_int64()
+        w = (C.c_int64 * (len(self.dims) - 1))()
+        b = (C.c_int64 * (len(self.dims) - 1))()
+        self._check(self._L.fdtd_mlp_layout(self._h, C.byref(n), w, b))
+        self.n_params = n.value
+        self.w_off, self.b_off = list(w), list(b)
+
+    def _check(self, st):
+        if st != 0:
+            raise FdtdError(st, self._L.fdtd_mlp_last_error(self._h).decode())
+
+    def layout(self):
+        """[(W offset, W shape (out, in), b offset)] per layer, within one member."""
+        return [(self.w_off[l], (self.dims[l + 1], self.dims[l]), self.b_off[l])
+                for l in range(len(self.dims) - 1)]
+
+    def unpack(self, flat):
+        """One member's flat parameters -> [(W, b)] per layer (views)."""
+        return [(flat[w:w + o * i].reshape(o, i), flat[b:b + o])
+                for w, (o, i), b in self.layout()]
+
+    def get_params(self):
+        out = np.empty((self.members, self.n_params), np.float32)
+        self._check(self._L.fdtd_mlp_get_params(self._h, _fp(out)))
+        return out
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32).reshape(self.members, self.n_params)
+        self._check(self._L.fdtd_mlp_set_params(self._h, _fp(p)))
+
+    def set_data(self, x, y):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.dims[0])
+        y = np.ascontiguousarray(y, np.float32).reshape(-1, self.dims[-1])
+        if len(x) != len(y):
+            raise ValueError("x and y differ in length")
+        self._check(self._L.fdtd_mlp_set_data(self._h, _fp(x), _fp(y), len(x)))
+
+    def grad(self, x, y):
+        """(loss [members], grads [members][n_params]) of every member on one batch."""
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.dims[0])
+        y = np.ascontiguousarray(y, np.float32).reshape(-1, self.dims[-1])
+        loss = np.empty(self.members, np.float32)
+        g = np.empty((self.members, self.n_params), np.float32)
+        self._check(self._L.fdtd_mlp_grad(self._h, _fp(x), _fp(y), len(x), _fp(loss), _fp(g)))
+        return loss, g
+
+    def train(self, epochs, batch=256, lr=1e-3, seed=0):
+        """Adam over the data of set_data(); returns the loss per epoch [epochs][members]."""
+        loss = np.empty((int(epochs), self.members), np.float32)
+        self._check(self._L.fdtd_mlp_train(self._h, int(epochs), int(batch), float(lr),
+                                           int(seed), _fp(loss)))
+        return loss
+
+    def predict(self, x, members=False):
+        """(mean, sd) over the ensemble, and every member's output when members=True."""
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.dims[0])
+        n, o = len(x), self.dims[-1]
+        mean = np.empty((n, o), np.float32)
+        sd = np.empty((n, o), np.float32)
+        per = np.empty((self.members, n, o), np.float32) if members else None
+        self._check(self._L.fdtd_mlp_predict(self._h, _fp(x), n, _fp(mean), _fp(sd),
+                                              None if per is None else _fp(per)))
+        return (mean, sd, per) if members else (mean, sd)
+
+    def predict_device(self, x_ptr, n, mean_ptr, sd_ptr, stream=None):
+        """predict() on device buffers (float32 pointers) ordered on `stream`."""
+        s = None
+        if stream is not None:
+            s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        self._check(self._L.fdtd_mlp_predict_device(self._h, C.c_void_p(x_ptr), int(n),
+                                                     C.c_void_p(mean_ptr), C.c_void_p(sd_ptr), s))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fdtd_mlp_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -896,6 +896,19 @@ fdtd_status fdtd_get_dft(fdtd_handle* h, int32_t monitor_id, double* re, double*
   return check_device_error(h);
 }
 
+fdtd_status fdtd_get_dft_device(fdtd_handle* h, int32_t monitor_id, double* re_dev,
+                                double* im_dev, void* stream) {
+  if (!h || monitor_id < 0 || monitor_id >= h->nmon || !re_dev || !im_dev)
+    return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  cudaStream_t st = pick_stream(h, stream);
+  const MonitorHost& m = h->mon[monitor_id];
+  const size_t bytes = (size_t)m.nf * h->g.nx * h->g.ny * sizeof(double);
+  CUDA_TRY(h, cudaMemcpyAsync(re_dev, m.re, bytes, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(h, cudaMemcpyAsync(im_dev, m.im, bytes, cudaMemcpyDeviceToDevice, st));
+  return FDTD_OK;
+}
+
 fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6) {
   if (!h || !scale6) return FDTD_ERR_INVALID_ARG;
   for (int c = 0; c < 6; ++c)

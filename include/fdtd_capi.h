@@ -160,6 +160,11 @@ fdtd_status fdtd_get_step(const fdtd_handle* h, int64_t* t);
 fdtd_status fdtd_get_field(fdtd_handle* h, int32_t component, float* host_out);
 fdtd_status fdtd_set_field(fdtd_handle* h, int32_t component, const float* host_in);
 fdtd_status fdtd_get_dft(fdtd_handle* h, int32_t monitor_id, double* re, double* im);
+/* Device-to-device copy of a monitor's running sums into [nf][Ny][Nx] double arrays on
+ * `stream` (a cudaStream_t or NULL for the handle's stream; asynchronous).  No reference
+ * counterpart: gDiamond reads its DFT sums on the host only. */
+fdtd_status fdtd_get_dft_device(fdtd_handle* h, int32_t monitor_id, double* re_dev,
+                                double* im_dev, void* stream);
 /* Device-to-device field copy into an unpitched Nx*Ny*Nz float array (asynchronous). */
 fdtd_status fdtd_get_field_device(fdtd_handle* h, int32_t component, float* dev_out,
                                   void* stream);
@@ -215,6 +220,45 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
  * launches in the last step, 1 if the last step replayed a graph}. */
 fdtd_status fdtd_batch_get_config(const fdtd_batch* b, int32_t* out6);
 const char* fdtd_batch_last_error(const fdtd_batch* b);
+
+/* ---------------------------------------------------------------- spectrum surrogate
+ * No reference counterpart (gDiamond has no learned component).  An ensemble of `members`
+ * MLPs dims[0] -> dims[1] -> ... -> dims[n_dims-1], GELU between layers, mean-squared-error
+ * loss, trained with Adam on the GPU.  FP32 master weights, BF16 GEMM operands, FP32
+ * accumulation on the tensor cores; all members run in the same launches.
+ *
+ * Parameter layout of one member (fdtd_mlp_layout): for every layer l, W_l row-major
+ * [dims[l+1]][dims[l]] at w_off[l] and b_l [dims[l+1]] at b_off[l] (blocks start on multiples
+ * of 8 floats; gaps are zero).  get/set_params move all members: [members][n_params]. */
+typedef struct fdtd_mlp fdtd_mlp;
+
+fdtd_status fdtd_mlp_create(const int32_t* dims, int32_t n_dims, int32_t members, uint64_t seed,
+                            int32_t device, fdtd_mlp** out);
+fdtd_status fdtd_mlp_destroy(fdtd_mlp* m);
+const char* fdtd_mlp_last_error(const fdtd_mlp* m);
+/* n_params per member; w_off / b_off (may be NULL) receive n_dims-1 offsets each. */
+fdtd_status fdtd_mlp_layout(const fdtd_mlp* m, int64_t* n_params, int64_t* w_off, int64_t* b_off);
+fdtd_status fdtd_mlp_get_params(fdtd_mlp* m, float* out);
+/* Replaces all members' parameters and restarts Adam. */
+fdtd_status fdtd_mlp_set_params(fdtd_mlp* m, const float* in);
+/* Training set (host): x [n][dims[0]], y [n][dims[last]], copied to the device. */
+fdtd_status fdtd_mlp_set_data(fdtd_mlp* m, const float* x, const float* y, int64_t n);
+/* Loss (mean squared error, per member) and gradient of every member on one batch (host x, y
+ * shared by all members); grads (may be NULL) [members][n_params]. */
+fdtd_status fdtd_mlp_grad(fdtd_mlp* m, const float* x, const float* y, int64_t n, float* loss,
+                          float* grads);
+/* `epochs` passes over the training set, minibatches of `batch` rows, every member its own
+ * shuffle per epoch (seeded), one Adam step (b1 0.9, b2 0.999, eps 1e-8) per minibatch.
+ * loss_out (may be NULL): [epochs][members] mean squared error over each epoch. */
+fdtd_status fdtd_mlp_train(fdtd_mlp* m, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                           float* loss_out);
+/* Ensemble mean and standard deviation over the members (host buffers, [n][dims[last]]);
+ * per_member (may be NULL) [members][n][dims[last]]. */
+fdtd_status fdtd_mlp_predict(fdtd_mlp* m, const float* x, int64_t n, float* mean, float* sd,
+                             float* per_member);
+/* The same on device buffers, ordered after and before work on `stream` (cudaStream_t). */
+fdtd_status fdtd_mlp_predict_device(fdtd_mlp* m, const float* x_dev, int64_t n, float* mean_dev,
+                                    float* sd_dev, void* stream);
 
 #ifdef __cplusplus
 }
