@@ -542,6 +542,106 @@ def run_batched(args):
     return 0
 
 
+def run_surrogate(args):
+    """Learned surrogate: 4096 training + 512 held-out designs (a dielectric box in a 96^3
+    grid, six numbers each), transmission spectra at 64 frequencies from the batched FP32 solver
+    (CUDA graph, T=2000); an ensemble of 4 MLPs 6->256->256->256->64 trained on the GPU
+    (BF16 tensor-core GEMMs, FP32 accumulation, Adam lr 1e-3, 200 epochs); held-out spectral
+    error against FDTD with and without the ensemble-disagreement fallback, and designs/s of
+    surrogate-with-fallback against the batched solver."""
+    import torch
+    from gdiamond_b200 import surrogate as S
+    T = args.timesteps if args.timesteps != T_STEPS else S.T_STEPS
+    sol = S.SpectrumSolver(T=T, group=256, observable=args.observable)
+    out = {}
+    if args.surrogate_data:
+        d = np.load(args.surrogate_data)
+        train, test = d["train"], d["test"]
+        y_train = sol.to_spectra(d["ex_train"], d["flux_train"])
+        y_test = sol.to_spectra(d["ex_test"], d["flux_test"])
+        sample = test[:256]  # the solver's rate, re-measured on part of the held-out set
+        y_s = sol.spectra(sample)
+        out["data"] = {"source": "loaded", "max_rel_diff_vs_loaded":
+                       float(S.spectral_error(y_s, y_test[:256]).max())}
+        solver_rate = len(sample) / sol.seconds
+    else:
+        train = S.sample_designs(args.train, seed=1)
+        test = S.sample_designs(args.test, seed=2)
+        t0 = time.perf_counter()
+        ex_tr, fl_tr = sol.measure(train)
+        t_gen = time.perf_counter() - t0
+        sol.seconds = 0.0
+        ex_te, fl_te = sol.measure(test)
+        solver_rate = len(test) / sol.seconds
+        y_train, y_test = sol.to_spectra(ex_tr, fl_tr), sol.to_spectra(ex_te, fl_te)
+        out["data"] = {"source": "generated", "train_seconds": t_gen}
+        if args.save_surrogate_data:
+            ex0, fl0 = sol.empty()
+            np.savez_compressed(args.save_surrogate_data, train=train, test=test,
+                                ex_train=ex_tr, flux_train=fl_tr, ex_test=ex_te,
+                                flux_test=fl_te, ex_empty=ex0, flux_empty=fl0, freqs=sol.freqs)
+    out["batched_solver"] = {"designs_per_s": solver_rate,
+                             "config": next(iter(sol.batches.values())).config()}
+    sur = S.Surrogate(members=4, seed=0)
+    t0 = time.perf_counter()
+    losses = sur.fit(train, y_train, epochs=args.epochs, batch=args.mlp_batch, lr=1e-3, seed=0)
+    t_fit = time.perf_counter() - t0
+    mean, sd = sur.predict(test)
+    err = S.spectral_error(mean, y_test)
+    dis = S.Surrogate.disagreement(mean, sd)
+    res = {}
+    for thr in (0.01, 0.02, 0.05):
+        spec, mask, t_s, t_f = sur.evaluate(test, sol, threshold=thr)
+        e = S.spectral_error(spec, y_test)
+        res[f"{thr:g}"] = {"fallback_fraction": float(mask.mean()),
+                           "designs_per_s": len(test) / (t_s + t_f),
+                           "speedup_vs_batched_solver": (len(test) / (t_s + t_f)) / solver_rate,
+                           "spectral_err_mean": float(e.mean()),
+                           "spectral_err_p95": float(np.quantile(e, 0.95)),
+                           "spectral_err_max": float(e.max())}
+    # inference throughput on device buffers (1M designs), CUDA events on the call's stream
+    n_inf = 1 << 20
+    x = torch.empty((n_inf, 6), device="cuda").uniform_(-1, 1)
+    m_ = torch.empty((n_inf, S.DIMS[-1]), device="cuda")
+    s_ = torch.empty_like(m_)
+    st = torch.cuda.current_stream()
+    for _ in range(3):
+        sur.net.predict_device(x.data_ptr(), n_inf, m_.data_ptr(), s_.data_ptr(), st)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    reps = 5
+    for _ in range(reps):
+        sur.net.predict_device(x.data_ptr(), n_inf, m_.data_ptr(), s_.data_ptr(), st)
+    e1.record(st)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3 / reps
+    dims = S.DIMS
+    flop = 2 * sum(a * b for a, b in zip(dims[:-1], dims[1:])) * 4 * n_inf
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    pk = json.load(open(pk_path)) if os.path.exists(pk_path) else {"bf16_tflops": 1590.0}
+    out["inference_1M"] = {"designs_per_s": n_inf / sec, "tflops": flop / sec / 1e12,
+                           "frac_of_bf16_peak": flop / sec / 1e12 / pk["bf16_tflops"]}
+    out["surrogate"] = {"observable": args.observable, "train_seconds": t_fit,
+                        "epochs": args.epochs, "batch": args.mlp_batch,
+                        "final_loss_per_member": [float(v) for v in losses[-1]],
+                        "heldout_err_mean_no_fallback": float(err.mean()),
+                        "heldout_err_median_no_fallback": float(np.median(err)),
+                        "heldout_err_p95_no_fallback": float(np.quantile(err, 0.95)),
+                        "baseline_mean_spectrum_err": float(S.spectral_error(
+                            np.broadcast_to(y_train.mean(0), y_test.shape), y_test).mean()),
+                        "disagreement_median": float(np.median(dis)),
+                        "with_fallback": res}
+    sur.close()
+    sol.close()
+    line = {"metric": "designs/s (surrogate with FDTD fallback vs batched solver) at stated "
+                      "held-out spectral error",
+            "workload": f"box designs in 96^3, T={T}, 64-freq transmission ({args.observable}), "
+                        f"{len(train)} train + {len(test)} held-out",
+            "results": out, "data": "synthetic (seeded designs)"}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -558,10 +658,21 @@ def main():
     ap.add_argument("--rows", type=int, default=0, help="force tile rows")
     ap.add_argument("--zchunks", type=int, default=0, help="force z-chunks")
     ap.add_argument("--min-blocks", type=int, default=0, help="force the register cap")
-    ap.add_argument("--workload", default="plain", choices=["plain", "mixed", "batched"],
+    ap.add_argument("--workload", default="plain",
+                    choices=["plain", "mixed", "batched", "surrogate"],
                     help="plain: the benchmark line; mixed / batched: the precision and "
                          "batching configurations (separate JSON lines)")
     ap.add_argument("--sims", type=int, default=64, help="batched workload: simulations")
+    ap.add_argument("--train", type=int, default=4096, help="surrogate: training designs")
+    ap.add_argument("--test", type=int, default=512, help="surrogate: held-out designs")
+    ap.add_argument("--epochs", type=int, default=200, help="surrogate: training epochs")
+    ap.add_argument("--mlp-batch", type=int, default=64, help="surrogate: minibatch rows")
+    ap.add_argument("--observable", default="flux", choices=["flux", "amplitude"],
+                    help="surrogate: transmission observable")
+    ap.add_argument("--surrogate-data", default="",
+                    help="surrogate: .npz of designs and measurements from an earlier run")
+    ap.add_argument("--save-surrogate-data", default="",
+                    help="surrogate: write the generated designs and measurements (.npz)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -569,6 +680,8 @@ def main():
         return run_mixed(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "surrogate":
+        return run_surrogate(args)
     return run_ours(args)
 
 

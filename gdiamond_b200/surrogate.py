@@ -12,12 +12,14 @@ The box is anti-aliased (a boundary cell gets eps = 1 + (eps-1) * covered volume
 the spectrum is a continuous function of the six numbers rather than a staircase in them.
 
 Excitation and observable: a current sheet on the interior of plane z = 10 driven by the
-Gaussian-modulated sinusoid of the point-source workloads launches a quasi-plane pulse along +z;
-the running DFT of E on plane z = 86 at 64 frequencies across the source band is summed over the
-plane (the normal-incidence amplitude), and the transmission spectrum is
-|S(f)|^2 / |S_empty(f)|^2 with S_empty from the same grid without the box.  The sheet current
-is transverse (Jx, observed on Ex): a z-directed current spread uniformly over a z-plane has
-zero curl and launches no wave along z.
+Gaussian-modulated sinusoid of the point-source workloads launches a quasi-plane pulse along +z.
+Running DFTs of Ex and Hy on plane z = 86 at 64 frequencies across the source band give the
+transmission spectrum as the z-flux through the plane, Sum Re(Ex conj(Hy)), divided by the same
+flux without the box ("flux"); the coherent normal-incidence amplitude |Sum Ex|^2 / |Sum
+Ex_empty|^2 is available as "amplitude".  (For this x-polarised pulse the Ey Hx* term of the
+flux is second order and is not recorded; the half-cell and half-step offsets of Hy from Ex
+cancel in the ratio to the empty grid.)  The sheet current is transverse (Jx): a z-directed
+current spread uniformly over a z-plane has zero curl and launches no wave along z.
 
 SpectrumSolver runs designs through the batched FDTD solver (the data generator, the fallback
 and the judge).  Surrogate wraps an ensemble of MLPs 6 -> 256 -> 256 -> 256 -> 64 (GELU, BF16
@@ -81,16 +83,20 @@ def design_eps(p, shape=SHAPE):
 class SpectrumSolver:
     """Transmission spectra of designs by batched FDTD (FP32 fields, FP64 DFT sums).
 
+    observable: "flux" (default) or "amplitude", as described in the module docstring.
+
     Simulations are created once (`group` of them) and reused: each group of designs gets new
     permittivities, a reset, and one persistent batched run of T steps replayed from a CUDA
     graph.
     """
 
     def __init__(self, shape=SHAPE, T=T_STEPS, n_freqs=N_FREQS, group=256, storage="f32",
-                 source_k=SOURCE_K, monitor_k=MONITOR_K, t_pml=10, device=0):
+                 source_k=SOURCE_K, monitor_k=MONITOR_K, t_pml=10, observable="flux", device=0):
         import torch
+        if observable not in ("flux", "amplitude"):
+            raise ValueError("observable is 'flux' or 'amplitude'")
         self.shape, self.T, self.group, self.storage = tuple(shape), int(T), int(group), storage
-        self.t_pml = int(t_pml)
+        self.t_pml, self.observable = int(t_pml), observable
         self.source_k, self.monitor_k, self.device = int(source_k), int(monitor_k), device
         self.freqs = W.source_band(n_freqs)
         self.wave = W.gaussian_wave(self.T)
@@ -100,39 +106,52 @@ class SpectrumSolver:
         nx, ny, _ = self.shape
         self._re = torch.empty((n_freqs, ny, nx), dtype=torch.float64, device=f"cuda:{device}")
         self._im = torch.empty_like(self._re)
-        self.seconds = 0.0  # wall time in plane_sums: permittivities, batched runs, read-back
+        self._hre = torch.empty_like(self._re)
+        self._him = torch.empty_like(self._re)
+        self.seconds = 0.0  # wall time in measure(): permittivities, batched runs, read-back
 
     def _make(self):
         sim = Simulation(*self.shape, storage=self.storage, device=self.device)
         sim.set_sources([dict(component="Jx", kind=SRC_PLANE_Z, k=self.source_k, wave=self.wave)])
         sim.add_dft_monitor("Ex", self.monitor_k, self.freqs)
+        sim.add_dft_monitor("Hy", self.monitor_k, self.freqs)
         return sim
 
-    def _plane_sums(self, sims):
+    def _measure(self, sims):
+        """[n][n_freqs] complex plane sums of Ex, and real z-fluxes Sum Re(Ex conj(Hy))."""
         import torch
-        out = np.empty((len(sims), len(self.freqs)), np.complex128)
+        nf = len(self.freqs)
+        ex = np.empty((len(sims), nf), np.complex128)
+        flux = np.empty((len(sims), nf), np.float64)
         stream = torch.cuda.current_stream(self.device)
         for n, sim in enumerate(sims):
             sim.get_dft_device(0, self._re.data_ptr(), self._im.data_ptr(), stream)
-            s = torch.stack((self._re.sum(dim=(1, 2)), self._im.sum(dim=(1, 2)))).cpu().numpy()
-            out[n] = s[0] + 1j * s[1]
-        return out
+            sim.get_dft_device(1, self._hre.data_ptr(), self._him.data_ptr(), stream)
+            r = torch.stack((self._re.sum(dim=(1, 2)), self._im.sum(dim=(1, 2)),
+                             (self._re * self._hre + self._im * self._him).sum(dim=(1, 2))))
+            r = r.cpu().numpy()
+            ex[n] = r[0] + 1j * r[1]
+            flux[n] = r[2]
+        return ex, flux
 
-    def empty_sum(self):
-        """Plane-summed DFT of the grid without a box (the normalisation)."""
+    def empty(self):
+        """(Ex plane sum, flux) of the grid without a box (the normalisation)."""
         if self._empty is None:
             sim = self._make()
             sim.set_permittivity(None, t_pml=self.t_pml)
             sim.step(self.T)
             sim.sync()
-            self._empty = self._plane_sums([sim])[0]
+            ex, flux = self._measure([sim])
+            self._empty = (ex[0], flux[0])
             sim.close()
         return self._empty
 
-    def plane_sums(self, designs):
-        """Complex plane-summed DFT [n][n_freqs] of every design."""
+    def measure(self, designs):
+        """(Ex plane sums [n][n_freqs] complex, fluxes [n][n_freqs]) of every design."""
         designs = np.asarray(designs, np.float32).reshape(-1, 6)
-        out = np.empty((len(designs), len(self.freqs)), np.complex128)
+        nf = len(self.freqs)
+        ex = np.empty((len(designs), nf), np.complex128)
+        flux = np.empty((len(designs), nf), np.float64)
         t0 = time.perf_counter()
         for g0 in range(0, len(designs), self.group):
             chunk = designs[g0:g0 + self.group]
@@ -150,13 +169,21 @@ class SpectrumSolver:
             b.step(self.T)
             for sim in sims:
                 sim.sync()
-            out[g0:g0 + len(chunk)] = self._plane_sums(sims)
+            e, f = self._measure(sims)
+            ex[g0:g0 + len(chunk)], flux[g0:g0 + len(chunk)] = e, f
         self.seconds += time.perf_counter() - t0
-        return out
+        return ex, flux
+
+    def to_spectra(self, ex, flux):
+        """Spectra [n][n_freqs] of measurements, by the solver's observable."""
+        ex0, flux0 = self.empty()
+        if self.observable == "flux":
+            return np.asarray(flux) / flux0[None, :]
+        return np.abs(np.asarray(ex) / ex0[None, :]) ** 2
 
     def spectra(self, designs):
-        """Transmission |S/S_empty|^2 [n][n_freqs] (float64)."""
-        return np.abs(self.plane_sums(designs) / self.empty_sum()[None, :]) ** 2
+        """Transmission spectra [n][n_freqs] (float64) of designs."""
+        return self.to_spectra(*self.measure(designs))
 
     def close(self):
         for b in self.batches.values():

@@ -1,8 +1,8 @@
 """The spectrum surrogate end to end on a small grid (32^3, T=300, 16 frequencies).
 
 * the batched FDTD spectrum solver (data generator, fallback, judge) against the oracle: the
-  plane-summed DFT of a design run in a batch equals the oracle's for the same permittivity,
-  and a box of eps 1 transmits exactly 1;
+  plane-summed Ex DFT and the z-flux of a design run in a batch equal the oracle's for the
+  same permittivity, and a box of eps 1 transmits exactly 1;
 * what the trained network gains over the method without it: on held-out designs the
   ensemble is far closer to FDTD than the best constant guess (the training-set mean), and
   the surrogate with fallback answers many times more designs per second than the batched
@@ -29,20 +29,25 @@ def test_solver_matches_oracle_and_unit_transmission():
     sol = solver(group=3)
     designs = S.sample_designs(3, seed=5, shape=SHAPE)
     designs[2, 5] = 1.0  # eps 1: the empty grid
-    sums = sol.plane_sums(designs)
-    for p, got in zip(designs[:2], sums[:2]):
+    ex, flux = sol.measure(designs)
+    for p, got_ex, got_flux in zip(designs[:2], ex[:2], flux[:2]):
         eps = S.design_eps(p, SHAPE)
         coefs = W.reference_coefficients(SHAPE, eps_re=eps, t_pml=PML)
-        mon = oracle.Monitor("Ex", MON_K, sol.freqs, 1.0)
+        me = oracle.Monitor("Ex", MON_K, sol.freqs, 1.0)
+        mh = oracle.Monitor("Hy", MON_K, sol.freqs, 1.0)
         oracle.run(SHAPE, coefs, T, sources=[oracle.Source("Jx", sol.wave, k=SRC_K,
                                                            kind=oracle.PLANE_Z)],
-                   monitors=[mon])
-        want = mon.re.sum(axis=(1, 2)) + 1j * mon.im.sum(axis=(1, 2))
-        assert np.abs(want).max() > 0
-        assert np.allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
-    spec = sol.spectra(designs)
-    assert np.allclose(spec[2], 1.0, rtol=0, atol=1e-12)  # S / S_empty up to the division
-    assert np.all(np.abs(spec[:2] - 1).max(axis=1) > 1e-3)  # a real box changes the spectrum
+                   monitors=[me, mh])
+        want_ex = me.re.sum(axis=(1, 2)) + 1j * me.im.sum(axis=(1, 2))
+        want_flux = (me.re * mh.re + me.im * mh.im).sum(axis=(1, 2))
+        assert np.abs(want_ex).max() > 0 and np.abs(want_flux).max() > 0
+        assert np.allclose(got_ex, want_ex, rtol=1e-12, atol=1e-12 * np.abs(want_ex).max())
+        assert np.allclose(got_flux, want_flux, rtol=1e-12, atol=1e-12 * np.abs(want_flux).max())
+    for obs in ("flux", "amplitude"):
+        sol.observable = obs
+        spec = sol.to_spectra(ex, flux)
+        assert np.allclose(spec[2], 1.0, rtol=0, atol=1e-12)  # up to the division
+        assert np.all(np.abs(spec[:2] - 1).max(axis=1) > 1e-3)  # a real box changes it
     sol.close()
 
 
