@@ -39,6 +39,7 @@ EXPORTS = (
     "fdtd_mlp_create", "fdtd_mlp_destroy", "fdtd_mlp_last_error", "fdtd_mlp_layout",
     "fdtd_mlp_get_params", "fdtd_mlp_set_params", "fdtd_mlp_set_data", "fdtd_mlp_grad",
     "fdtd_mlp_train", "fdtd_mlp_predict", "fdtd_mlp_predict_device", "fdtd_get_dft_device",
+    "fdtd_mlp_set_gemm",
 )
 
 
@@ -117,6 +118,7 @@ def library():
             "fdtd_mlp_predict": ([V, P(C.c_float), C.c_int64, P(C.c_float), P(C.c_float),
                                   P(C.c_float)], C.c_int),
             "fdtd_mlp_predict_device": ([V, V, C.c_int64, V, V, V], C.c_int),
+            "fdtd_mlp_set_gemm": ([V, C.c_int32], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -383,7 +385,9 @@ class MLP:
     [members][n_params]; ``layout()`` gives each layer's weight and bias offsets.
     """
 
-    def __init__(self, dims, members=4, seed=0, device=0):
+    GEMMS = {"tcgen05": 0, "mma_sync": 1}
+
+    def __init__(self, dims, members=4, seed=0, device=0, gemm="tcgen05"):
         self.dims = tuple(int(d) for d in dims)
         self.members = int(members)
         self._L = library()
@@ -400,6 +404,12 @@ class MLP:
         self._check(self._L.fdtd_mlp_layout(self._h, C.byref(n), w, b))
         self.n_params = n.value
         self.w_off, self.b_off = list(w), list(b)
+        self.set_gemm(gemm)
+
+    def set_gemm(self, gemm):
+        """GEMM path: "tcgen05" (tensor-memory accumulator) or "mma_sync" (warp-level)."""
+        self._check(self._L.fdtd_mlp_set_gemm(self._h, self.GEMMS[gemm]))
+        self.gemm = gemm
 
     def _check(self, st):
         if st != 0:

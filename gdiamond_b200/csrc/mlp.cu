@@ -6,14 +6,17 @@
 //
 // Network per member: x -> [Linear -> GELU] x (L-1) -> Linear -> y, mean-squared-error loss.
 // FP32 master weights (updated by Adam) and BF16 copies (the GEMM operands); activations that
-// feed a GEMM are BF16; every GEMM accumulates in FP32 on the tensor cores
-// (mma.sync.m16n8k16 BF16).  All members of the ensemble run in the same launches
-// (blockIdx.z = member), each on its own minibatch.
+// feed a GEMM are BF16; every GEMM accumulates in FP32 on the tensor cores.  All members of the
+// ensemble run in the same launches (blockIdx.z = member), each on its own minibatch.
+//
+// Two GEMM paths compute the same products: tcgen05.mma with a TMEM accumulator (mlp_tc.cu, the
+// default) and the warp-level mma.sync.m16n8k16 kernel below (selectable with
+// fdtd_mlp_set_gemm; the cross-check of the first).
 //
 // GEMM: C[M][N] = sum_k opA(m,k) opB(n,k), opX(r,k) = TX ? X[k*ld + r] : X[r*ld + k], so one
 // kernel serves the forward pass (X W^T), the input gradient (G W) and the weight gradient
-// (G^T X).  64x64 CTA tiles (4 warps of 32x32), K in steps of 32 with the next step's tile
-// prefetched into registers, zero fill outside the matrices, and fused epilogues:
+// (G^T X).  mma.sync path: 64x64 CTA tiles (4 warps of 32x32), K in steps of 32 with the next
+// step's tile prefetched into registers, zero fill outside the matrices.  Fused epilogues:
 //   kStore      C = acc                                   (weight gradients)
 //   kBias       Z = acc + b                               (output layer)
 //   kBiasGelu   Z = acc + b, A = bf16(GELU(Z))            (hidden layers)
@@ -32,29 +35,12 @@
 #include <vector>
 
 #include "../../include/fdtd_capi.h"
+#include "mlp.cuh"
 
 namespace fdtd {
 namespace mlp {
 
 constexpr int BM = 64, BN = 64, BK = 32, KP = BK + 8;  // smem row: 32 bf16 + 8 pad (80 B)
-enum Epi { kStore = 0, kBias = 1, kBiasGelu = 2, kGeluBack = 3 };
-
-struct Operand {
-  const __nv_bfloat16* p;
-  int ld;
-  long long stride;  // per member (elements); 0 = shared by all members
-  bool vec;          // 16-byte loads allowed (ld, stride multiples of 8, base 16-byte aligned)
-};
-
-struct Epilogue {
-  float* out;              // C (kStore), Z (kBias, kBiasGelu), G (kGeluBack)
-  __nv_bfloat16* out_bf;   // A (kBiasGelu), Gbf (kGeluBack)
-  const float* bias;       // kBias, kBiasGelu
-  const float* zp;         // kGeluBack: pre-activation of the layer below, same shape as out
-  int ldc;
-  long long stride_out, stride_bias, stride_zp;
-};
-
 // One thread's share of a 64 x 32 tile of op(X): two 16-byte chunks of 8 elements.
 struct Chunk {
   uint4 v[2];
@@ -110,15 +96,6 @@ __device__ __forceinline__ void store_tile(__nv_bfloat16 (*s)[KP], const Chunk& 
       for (int q = 0; q < 8; ++q) s[r + q][kk] = e[q];
     }
   }
-}
-
-// GELU with the exact (erf) form and its derivative.
-__device__ __forceinline__ float gelu(float z) {
-  return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
-}
-__device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) +
-         z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
 template <bool TA, bool TB, int EPI>
@@ -183,7 +160,6 @@ __global__ void __launch_bounds__(128) gemm_bf16(int M, int N, int K, Operand A,
     __syncthreads();
   }
 
-  float* out = ep.out + e * ep.stride_out;
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -195,14 +171,7 @@ __global__ void __launch_bounds__(128) gemm_bf16(int M, int N, int K, Operand A,
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
           const int c = n0 + wn + j * 8 + tig * 2 + q;
-          if (c >= N) continue;
-          const long long o = (long long)r * ep.ldc + c;
-          float v = acc[i][j][h * 2 + q];
-          if (EPI == kBias || EPI == kBiasGelu) v += ep.bias[e * ep.stride_bias + c];
-          if (EPI == kGeluBack) v *= gelu_grad(ep.zp[e * ep.stride_zp + o]);
-          out[o] = v;
-          if (EPI == kBiasGelu) ep.out_bf[e * ep.stride_out + o] = __float2bfloat16_rn(gelu(v));
-          if (EPI == kGeluBack) ep.out_bf[e * ep.stride_out + o] = __float2bfloat16_rn(v);
+          if (c < N) epilogue_store<EPI>(ep, e, r, c, acc[i][j][h * 2 + q]);
         }
       }
 }
@@ -324,6 +293,9 @@ struct fdtd_mlp {
   __nv_bfloat16* gbf[2] = {nullptr, nullptr};  // their BF16 copies
   float* tgt = nullptr;                        // [E][cap][out]
   float* xin = nullptr;                        // FP32 input staging [cap][in]
+  int gemm_kind = FDTD_MLP_GEMM_TCGEN05;
+  mutable cudaError_t launch_err = cudaSuccess;  // first failed tcgen05 launch set-up
+  int* d_err = nullptr;  // nonzero when a bounded wait in a GEMM kernel gave up
   std::string err;
 };
 
@@ -388,9 +360,35 @@ Operand operand(const __nv_bfloat16* p, int ld, long long stride) {
 template <bool TA, bool TB, int EPI>
 void gemm(const fdtd_mlp* m, int M, int N, int K, const Operand& A, const Operand& B,
           const Epilogue& ep) {
+  if (m->gemm_kind == FDTD_MLP_GEMM_TCGEN05) {
+    const cudaError_t e =
+        fdtd::mlp::launch_gemm_tc<TA, TB, EPI>(M, N, K, A, B, ep, m->E, m->st, m->d_err);
+    if (e != cudaSuccess && m->launch_err == cudaSuccess) m->launch_err = e;
+    return;
+  }
   const dim3 grid((N + fdtd::mlp::BN - 1) / fdtd::mlp::BN, (M + fdtd::mlp::BM - 1) / fdtd::mlp::BM,
                   m->E);
   fdtd::mlp::gemm_bf16<TA, TB, EPI><<<grid, 128, 0, m->st>>>(M, N, K, A, B, ep);
+}
+
+// After a synchronisation: launch errors and the GEMMs' device error word.
+fdtd_status check_after(fdtd_mlp* m) {
+  if (m->launch_err != cudaSuccess) {
+    const cudaError_t le = m->launch_err;
+    m->launch_err = cudaSuccess;
+    return mfail(m, FDTD_ERR_CUDA, cudaGetErrorString(le));
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return mfail(m, FDTD_ERR_CUDA, cudaGetErrorString(e));
+  int w = 0;
+  if (cudaMemcpy(&w, m->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return mfail(m, FDTD_ERR_CUDA, "reading the device error word failed");
+  if (w) {
+    cudaMemset(m->d_err, 0, sizeof(int));
+    return mfail(m, FDTD_ERR_DEVICE_TIMEOUT,
+                 "a bounded wait in a tensor-core GEMM expired; results are invalid");
+  }
+  return FDTD_OK;
 }
 
 // Forward pass of every member on M rows of act[0] (member stride act0_stride; 0 when all
@@ -464,6 +462,7 @@ void destroy(fdtd_mlp* m) {
   cudaFree(m->adam_m);
   cudaFree(m->adam_v);
   cudaFree(m->wbf);
+  cudaFree(m->d_err);
   cudaFree(m->X);
   cudaFree(m->Y);
   if (m->st) cudaStreamDestroy(m->st);
@@ -528,7 +527,9 @@ fdtd_status fdtd_mlp_create(const int32_t* dims, int32_t n_dims, int32_t members
       cudaMalloc(&m->grads, tot * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&m->adam_m, tot * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&m->adam_v, tot * sizeof(float)) != cudaSuccess ||
-      cudaMalloc(&m->wbf, tot * sizeof(__nv_bfloat16)) != cudaSuccess) {
+      cudaMalloc(&m->wbf, tot * sizeof(__nv_bfloat16)) != cudaSuccess ||
+      cudaMalloc(&m->d_err, sizeof(int)) != cudaSuccess ||
+      cudaMemset(m->d_err, 0, sizeof(int)) != cudaSuccess) {
     destroy(m);
     return FDTD_ERR_OOM;
   }
@@ -556,6 +557,13 @@ fdtd_status fdtd_mlp_create(const int32_t* dims, int32_t n_dims, int32_t members
     return FDTD_ERR_CUDA;
   }
   *out = m;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_mlp_set_gemm(fdtd_mlp* m, int32_t kind) {
+  if (!m || (kind != FDTD_MLP_GEMM_TCGEN05 && kind != FDTD_MLP_GEMM_MMA_SYNC))
+    return FDTD_ERR_INVALID_ARG;
+  m->gemm_kind = kind;
   return FDTD_OK;
 }
 
@@ -638,6 +646,7 @@ fdtd_status fdtd_mlp_grad(fdtd_mlp* m, const float* x, const float* y, int64_t n
   const cudaError_t e = cudaStreamSynchronize(m->st);
   cudaFree(dloss);
   if (e != cudaSuccess) return mfail(m, FDTD_ERR_CUDA, cudaGetErrorString(e));
+  if ((s = check_after(m)) != FDTD_OK) return s;
   if (loss)
     for (int i = 0; i < m->E; ++i) loss[i] = (float)((double)hl[i] / ((double)n * out));
   return FDTD_OK;
@@ -697,6 +706,7 @@ fdtd_status fdtd_mlp_train(fdtd_mlp* m, int32_t epochs, int32_t batch, float lr,
   cudaFree(dloss);
   if (err != cudaSuccess) return mfail(m, FDTD_ERR_CUDA, cudaGetErrorString(err));
   if (e2 != cudaSuccess) return mfail(m, FDTD_ERR_CUDA, cudaGetErrorString(e2));
+  if ((s = check_after(m)) != FDTD_OK) return s;
   if (loss_out)
     for (size_t i = 0; i < hl.size(); ++i) loss_out[i] = (float)((double)hl[i] / ((double)n * out));
   return FDTD_OK;
@@ -730,7 +740,7 @@ fdtd_status fdtd_mlp_predict(fdtd_mlp* m, const float* x, int64_t n, float* mean
   if (s != FDTD_OK) return s;
   if (e != cudaSuccess) return mfail(m, FDTD_ERR_CUDA, cudaGetErrorString(e));
   if (e2 != cudaSuccess) return mfail(m, FDTD_ERR_CUDA, cudaGetErrorString(e2));
-  return FDTD_OK;
+  return check_after(m);
 }
 
 fdtd_status fdtd_mlp_predict_device(fdtd_mlp* m, const float* x_dev, int64_t n, float* mean_dev,

@@ -1,0 +1,58 @@
+// mlp.cuh -- definitions shared by the surrogate MLP's GEMM kernels (mlp.cu: mma.sync family
+// and host code; mlp_tc.cu: tcgen05 / TMEM family).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fdtd {
+namespace mlp {
+
+enum Epi { kStore = 0, kBias = 1, kBiasGelu = 2, kGeluBack = 3 };
+
+// op(X)(r, k) = T ? X[k*ld + r] : X[r*ld + k] (+ member * stride)
+struct Operand {
+  const __nv_bfloat16* p;
+  int ld;
+  long long stride;  // per member (elements); 0 = shared by all members
+  bool vec;          // 16-byte loads allowed (ld, stride multiples of 8, base 16-byte aligned)
+};
+
+struct Epilogue {
+  float* out;              // C (kStore), Z (kBias, kBiasGelu), G (kGeluBack)
+  __nv_bfloat16* out_bf;   // A (kBiasGelu), Gbf (kGeluBack)
+  const float* bias;       // kBias, kBiasGelu
+  const float* zp;         // kGeluBack: pre-activation of the layer below, same shape as out
+  int ldc;
+  long long stride_out, stride_bias, stride_zp;
+};
+
+// GELU with the exact (erf) form and its derivative.
+__device__ __forceinline__ float gelu(float z) {
+  return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) +
+         z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+// The fused epilogue of one accumulator element (member e, row r, column c).
+template <int EPI>
+__device__ __forceinline__ void epilogue_store(const Epilogue& ep, int e, int r, int c, float v) {
+  const long long o = (long long)r * ep.ldc + c;
+  if (EPI == kBias || EPI == kBiasGelu) v += ep.bias[e * ep.stride_bias + c];
+  if (EPI == kGeluBack) v *= gelu_grad(ep.zp[e * ep.stride_zp + o]);
+  ep.out[e * ep.stride_out + o] = v;
+  if (EPI == kBiasGelu) ep.out_bf[e * ep.stride_out + o] = __float2bfloat16_rn(gelu(v));
+  if (EPI == kGeluBack) ep.out_bf[e * ep.stride_out + o] = __float2bfloat16_rn(v);
+}
+
+// tcgen05 GEMM (mlp_tc.cu): C[M][N] (+epilogue) for `members` members on `st`; `err` receives
+// a nonzero word if a bounded wait inside the kernel gave up.
+template <bool TA, bool TB, int EPI>
+cudaError_t launch_gemm_tc(int M, int N, int K, const Operand& A, const Operand& B,
+                           const Epilogue& ep, int members, cudaStream_t st, int* err);
+
+}  // namespace mlp
+}  // namespace fdtd

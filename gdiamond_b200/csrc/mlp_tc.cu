@@ -1,0 +1,285 @@
+// mlp_tc.cu -- the surrogate MLP's GEMMs on the 5th-generation tensor cores (tcgen05 + TMEM).
+//
+// C[M][N] = sum_k opA(m,k) opB(n,k) with BF16 operands and an FP32 accumulator held in tensor
+// memory, followed by the fused epilogues of mlp.cuh.  One CTA = 4 warps computes a 128 x BN
+// tile (BN = 64 or 128) for one ensemble member (blockIdx.z):
+//   - K advances in 64-wide steps through two shared-memory stages.  All 128 threads stage a
+//     step's A (128 x 64) and B (BN x 64) tiles from global memory, transposing where the
+//     operand is stored k-major, into the no-swizzle K-major "core matrix" layout the tensor
+//     core reads (8 rows x 16 bytes contiguous; the two 8-element halves of a K=16 slice 128 B
+//     apart, 8-row groups 1024 B apart).
+//   - One thread issues four tcgen05.mma (M=128, N=BN, K=16 each) per step and commits them to
+//     the stage's mbarrier; the next step's staging overlaps them, and a stage is refilled only
+//     after its commit arrives.
+//   - The accumulator (BN FP32 columns x 128 lanes) is allocated in TMEM by warp 0 and read back
+//     with tcgen05.ld (warp w owns lanes 32w..32w+31 = tile rows), 16 columns at a time, into
+//     the epilogue.
+// Every mbarrier wait is bounded; on expiry the kernel records an error word, stops issuing
+// (decided block-wide with __syncthreads_or), waits (bounded) for what it issued, skips the
+// epilogue, frees its TMEM and returns.
+#include "fdtd_common.cuh"
+#include "mlp.cuh"
+
+namespace fdtd {
+namespace mlp {
+namespace {
+
+constexpr int TBM = 128, TBK = 64;
+constexpr long long kTcWaitLimit = 2000000000LL;  // SM clocks, ~1 s
+
+// Byte offset of element (r, k) of an R x 64 tile in the core-matrix layout.
+__device__ __forceinline__ uint32_t cm_off(int r, int k) {
+  return (uint32_t)(((((r >> 3) * (TBK / 8)) + (k >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+// Shared-memory matrix descriptor: start address, leading byte offset (between the K halves:
+// 128 B), stride byte offset (between 8-row groups: 1024 B), descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
+  const uint64_t lbo = 128 >> 4, sbo = ((TBK / 8) * 128) >> 4;
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, N, M=128.
+template <int BN>
+__host__ __device__ constexpr uint32_t instr_desc() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)(TBM >> 4) << 24);
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(slot)),
+               "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc,
+                                          uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Stages rows [r0, r0+R) x k [k0, k0+64) of op(X) into the core-matrix tile at s (zeros outside
+// the R_tot x K matrix).
+template <bool T, int R>
+__device__ __forceinline__ void stage_tile(uint8_t* s, const Operand& X, const __nv_bfloat16* base,
+                                           int R_tot, int K, int r0, int k0) {
+  const int tid = threadIdx.x;
+  const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+#pragma unroll
+  for (int it = 0; it < R * 8 / 128; ++it) {
+    const int id = tid + it * 128;
+    if (!T) {
+      // 8 consecutive k of one row; a warp writes 4 whole core matrices (512 contiguous bytes)
+      const int r = (id >> 6) * 8 + (id & 7), k = ((id >> 3) & 7) * 8;
+      const int gr = r0 + r, gk = k0 + k;
+      uint4 v;
+      if (X.vec && gr < R_tot && gk + 8 <= K) {
+        v = *reinterpret_cast<const uint4*>(base + (long long)gr * X.ld + gk);
+      } else {
+        __nv_bfloat16 e[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          e[q] = (gr < R_tot && gk + q < K) ? base[(long long)gr * X.ld + gk + q] : zero;
+        memcpy(&v, e, 16);
+      }
+      *reinterpret_cast<uint4*>(s + cm_off(r, k)) = v;
+    } else {
+      // 8 consecutive rows at one k (contiguous in memory), scattered to 8 rows of the tile
+      const int r = (id % (R / 8)) * 8, k = id / (R / 8);
+      const int gr = r0 + r, gk = k0 + k;
+      __nv_bfloat16 e[8];
+      if (X.vec && gk < K && gr + 8 <= R_tot) {
+        const uint4 v = *reinterpret_cast<const uint4*>(base + (long long)gk * X.ld + gr);
+        memcpy(e, &v, 16);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          e[q] = (gk < K && gr + q < R_tot) ? base[(long long)gk * X.ld + gr + q] : zero;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) *reinterpret_cast<__nv_bfloat16*>(s + cm_off(r + q, k)) = e[q];
+    }
+  }
+}
+
+template <int BN>
+struct TcSmem {
+  static constexpr uint32_t A_BYTES = TBM * TBK * 2;
+  static constexpr uint32_t B_BYTES = BN * TBK * 2;
+  static constexpr uint32_t OFF_B = 2 * A_BYTES;
+  static constexpr uint32_t OFF_BAR = OFF_B + 2 * B_BYTES;
+  static constexpr uint32_t BYTES = OFF_BAR + 64 + 1024;  // + barriers, slots, alignment slack
+};
+
+template <bool TA, bool TB, int EPI, int BN>
+__global__ void __launch_bounds__(128) gemm_tc(int M, int N, int K, Operand A, Operand B,
+                                               Epilogue ep, int* err) {
+  using L = TcSmem<BN>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                           ~static_cast<uintptr_t>(1023));
+  uint8_t* sA = sm;
+  uint8_t* sB = sm + L::OFF_B;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + L::OFF_BAR);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int e = blockIdx.z;
+  const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * BN;
+  const __nv_bfloat16* Ab = A.p + e * A.stride;
+  const __nv_bfloat16* Bb = B.p + e * B.stride;
+
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, BN);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  const int nk = (K + TBK - 1) / TBK;
+  int issued = 0;  // K steps whose MMAs were issued and committed
+  bool aborted = false;
+  for (int kt = 0; kt < nk; ++kt) {
+    const int s = kt & 1;
+    bool bad = false;
+    if (kt >= 2 && !mbar_wait_bounded(&bar[s], ((kt - 2) >> 1) & 1, kTcWaitLimit)) {
+      bad = true;
+      atomicExch(err, 1);
+    }
+    if (!bad) {
+      stage_tile<TA, TBM>(sA + s * L::A_BYTES, A, Ab, M, K, m0, kt * TBK);
+      stage_tile<TB, BN>(sB + s * L::B_BYTES, B, Bb, N, K, n0, kt * TBK);
+    }
+    fence_proxy_async_smem();
+    if (__syncthreads_or(bad)) {  // a barrier whose result every thread shares
+      aborted = true;
+      break;
+    }
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(sA + s * L::A_BYTES), b0 = smem_u32(sB + s * L::B_BYTES);
+#pragma unroll
+      for (int j = 0; j < TBK / 16; ++j)
+        umma_bf16(tmem, smem_desc(a0 + j * 256), smem_desc(b0 + j * 256), instr_desc<BN>(),
+                  (kt > 0 || j > 0) ? 1u : 0u);
+      umma_commit(&bar[s]);
+    }
+    issued = kt + 1;
+  }
+  // The last commit arrives once every MMA issued before it has completed.
+  bool late = false;
+  if (issued > 0) {
+    const int last = issued - 1;
+    late = !mbar_wait_bounded(&bar[last & 1], (last >> 1) & 1, kTcWaitLimit);
+    if (late) atomicExch(err, 1);
+  }
+  late = __syncthreads_or(late);
+  tc_fence_after();
+  if (!late && !aborted && issued > 0) {
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN && n0 + c0 < N; c0 += 16) {
+      uint32_t v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      tmem_wait_ld();
+      if (row < M) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int c = n0 + c0 + q;
+          if (c < N) epilogue_store<EPI>(ep, e, row, c, __uint_as_float(v[q]));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, BN);
+}
+
+template <bool TA, bool TB, int EPI, int BN>
+cudaError_t launch_bn(int M, int N, int K, const Operand& A, const Operand& B, const Epilogue& ep,
+                      int members, cudaStream_t st, int* err) {
+  static unsigned long long set_on = 0;  // devices (bit per ordinal < 64) with the attribute set
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+  if (!(set_on & bit) || !bit) {
+    e = cudaFuncSetAttribute(gemm_tc<TA, TB, EPI, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TcSmem<BN>::BYTES);
+    if (e != cudaSuccess) return e;
+    set_on |= bit;
+  }
+  const dim3 grid((N + BN - 1) / BN, (M + TBM - 1) / TBM, members);
+  gemm_tc<TA, TB, EPI, BN><<<grid, 128, TcSmem<BN>::BYTES, st>>>(M, N, K, A, B, ep, err);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+template <bool TA, bool TB, int EPI>
+cudaError_t launch_gemm_tc(int M, int N, int K, const Operand& A, const Operand& B,
+                           const Epilogue& ep, int members, cudaStream_t st, int* err) {
+  if (M < 1 || N < 1 || K < 1 || members < 1) return cudaErrorInvalidValue;
+  if (N <= 64) return launch_bn<TA, TB, EPI, 64>(M, N, K, A, B, ep, members, st, err);
+  return launch_bn<TA, TB, EPI, 128>(M, N, K, A, B, ep, members, st, err);
+}
+
+// The instances the MLP uses: forward (X W^T), weight gradient (G^T X), input gradient (G W).
+template cudaError_t launch_gemm_tc<false, false, kBiasGelu>(int, int, int, const Operand&,
+                                                             const Operand&, const Epilogue&, int,
+                                                             cudaStream_t, int*);
+template cudaError_t launch_gemm_tc<false, false, kBias>(int, int, int, const Operand&,
+                                                         const Operand&, const Epilogue&, int,
+                                                         cudaStream_t, int*);
+template cudaError_t launch_gemm_tc<true, true, kStore>(int, int, int, const Operand&,
+                                                        const Operand&, const Epilogue&, int,
+                                                        cudaStream_t, int*);
+template cudaError_t launch_gemm_tc<false, true, kGeluBack>(int, int, int, const Operand&,
+                                                            const Operand&, const Epilogue&, int,
+                                                            cudaStream_t, int*);
+
+}  // namespace mlp
+}  // namespace fdtd

@@ -232,10 +232,18 @@ const char* fdtd_batch_last_error(const fdtd_batch* b);
  * of 8 floats; gaps are zero).  get/set_params move all members: [members][n_params]. */
 typedef struct fdtd_mlp fdtd_mlp;
 
+/* GEMM path of an ensemble: tcgen05.mma with the accumulator in tensor memory (default), or the
+ * warp-level mma.sync kernel (the same products; kept as a cross-check). */
+typedef enum fdtd_mlp_gemm {
+  FDTD_MLP_GEMM_TCGEN05 = 0,
+  FDTD_MLP_GEMM_MMA_SYNC = 1
+} fdtd_mlp_gemm;
+
 fdtd_status fdtd_mlp_create(const int32_t* dims, int32_t n_dims, int32_t members, uint64_t seed,
                             int32_t device, fdtd_mlp** out);
 fdtd_status fdtd_mlp_destroy(fdtd_mlp* m);
 const char* fdtd_mlp_last_error(const fdtd_mlp* m);
+fdtd_status fdtd_mlp_set_gemm(fdtd_mlp* m, int32_t kind);
 /* n_params per member; w_off / b_off (may be NULL) receive n_dims-1 offsets each. */
 fdtd_status fdtd_mlp_layout(const fdtd_mlp* m, int64_t* n_params, int64_t* w_off, int64_t* b_off);
 fdtd_status fdtd_mlp_get_params(fdtd_mlp* m, float* out);

@@ -1,7 +1,9 @@
 """The surrogate's GPU MLP ensemble (fdtd_mlp_*) against the CPU FP64 oracle (oracle/mlp.py).
 
 * gradients of every member (BF16 tensor-core GEMMs, FP32 accumulation) against the oracle
-  with the same BF16 roundings (tight) and against exact FP64 backprop (loose);
+  with the same BF16 roundings (tight) and against exact FP64 backprop (loose), for both GEMM
+  paths (tcgen05 with a TMEM accumulator, and warp-level mma.sync), and the two paths against
+  each other on odd shapes;
 * forward outputs of every member and the ensemble mean / standard deviation;
 * one Adam step against the oracle's Adam on the oracle's gradient;
 * training on a smooth function lowers the loss and generalises; invalid arguments fail.
@@ -25,10 +27,29 @@ def data(n, dims, seed):
             rng.normal(0, 1, (n, dims[-1])).astype(np.float32))
 
 
+@pytest.mark.parametrize("dims,members,n", [((6, 37, 19, 3), 2, 70), ((7, 200, 130, 72), 3, 333),
+                                            ((6, 256, 256, 256, 64), 4, 1000)])
+def test_gemm_paths_agree(dims, members, n):
+    x, y = data(n, dims, 9)
+    out = {}
+    for gemm in ("mma_sync", "tcgen05"):
+        net = gd.MLP(dims, members=members, seed=5, gemm=gemm)
+        mean, sd, per = net.predict(x, members=True)
+        loss, g = net.grad(x, y)
+        out[gemm] = (per, loss, g)
+        net.close()
+    (p0, l0, g0), (p1, l1, g1) = out["mma_sync"], out["tcgen05"]
+    assert rel(p1, p0) <= 1e-4, rel(p1, p0)
+    assert np.allclose(l1, l0, rtol=1e-4)
+    for e in range(members):
+        assert rel(g1[e], g0[e]) <= 2e-3, (e, rel(g1[e], g0[e]))
+
+
+@pytest.mark.parametrize("gemm", ["tcgen05", "mma_sync"])
 @pytest.mark.parametrize("dims,members,n", [((6, 256, 256, 256, 64), 4, 200),
                                             ((5, 37, 19, 3), 2, 70)])
-def test_gradients_match_oracle(dims, members, n):
-    net = gd.MLP(dims, members=members, seed=7)
+def test_gradients_match_oracle(dims, members, n, gemm):
+    net = gd.MLP(dims, members=members, seed=7, gemm=gemm)
     x, y = data(n, dims, 1)
     loss, g = net.grad(x, y)
     P = net.get_params()
@@ -47,9 +68,10 @@ def test_gradients_match_oracle(dims, members, n):
     net.close()
 
 
-def test_forward_and_ensemble_statistics_match_oracle():
+@pytest.mark.parametrize("gemm", ["tcgen05", "mma_sync"])
+def test_forward_and_ensemble_statistics_match_oracle(gemm):
     dims = (6, 256, 256, 256, 64)
-    net = gd.MLP(dims, members=4, seed=3)
+    net = gd.MLP(dims, members=4, seed=3, gemm=gemm)
     x, _ = data(333, dims, 2)
     mean, sd, per = net.predict(x, members=True)
     P = net.get_params()
@@ -137,6 +159,8 @@ def test_invalid_arguments():
     net = gd.MLP((4, 8, 2), members=1)
     with pytest.raises(gd.FdtdError):
         net.train(epochs=1)  # no data
+    with pytest.raises(KeyError):
+        net.set_gemm("wmma")
     with pytest.raises(ValueError):
         net.set_data(np.zeros((3, 4)), np.zeros((2, 2)))
     net.close()
