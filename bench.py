@@ -474,9 +474,9 @@ def run_batched(args):
     wave = W.gaussian_wave(T)
     total_cells = sum(int(np.prod(s[0])) for s in specs)
 
-    def make(spec, storage, scales=None):
+    def make(spec, storage, scales=None, blt=0):
         shape, eps, pos = spec
-        sim = gd.Simulation(*shape, storage=storage)
+        sim = gd.Simulation(*shape, storage=storage, blt=blt)
         if scales is not None:
             sim.set_storage_scale(scales)
         sim.set_permittivity(eps)
@@ -509,9 +509,9 @@ def run_batched(args):
     shape0, _, pos0 = specs[small]
     f16 = fp16_scales(make((shape0, np.ones(int(np.prod(shape0)), np.float32), pos0), "f32"),
                       int(np.prod(shape0)), min(T, 300))
-    for storage in ("bf16", "f16"):
+    for storage in args.batch_storage.split(","):
         scales = f16 if storage == "f16" else None
-        sims = [make(sp, storage, scales) for sp in specs]
+        sims = [make(sp, storage, scales, blt=args.blt) for sp in specs]
         batch = gd.Batch(sims)
         batch.step(4)  # batch autotune outside the timed region
         for s in sims:
@@ -560,7 +560,9 @@ def run_surrogate(args):
         y_train = sol.to_spectra(d["ex_train"], d["flux_train"])
         y_test = sol.to_spectra(d["ex_test"], d["flux_test"])
         sample = test[:256]  # the solver's rate, re-measured on part of the held-out set
-        y_s = sol.spectra(sample)
+        y_s = sol.spectra(sample)  # first call: creates the simulations, tunes, captures
+        sol.seconds = 0.0
+        sol.spectra(sample)
         out["data"] = {"source": "loaded", "max_rel_diff_vs_loaded":
                        float(S.spectral_error(y_s, y_test[:256]).max())}
         solver_rate = len(sample) / sol.seconds
@@ -591,6 +593,7 @@ def run_surrogate(args):
     dis = S.Surrogate.disagreement(mean, sd)
     res = {}
     for thr in (0.01, 0.02, 0.05):
+        sur.evaluate(test, sol, threshold=thr)  # warm: batches of this fallback size exist
         spec, mask, t_s, t_f = sur.evaluate(test, sol, threshold=thr)
         e = S.spectral_error(spec, y_test)
         res[f"{thr:g}"] = {"fallback_fraction": float(mask.mean()),
@@ -642,6 +645,59 @@ def run_surrogate(args):
     return 0
 
 
+def run_mlp(args):
+    """The surrogate's tensor-core GEMMs alone: ensemble inference (4 members, 6->256->256->256
+    ->64, BF16 operands, FP32 accumulation) on `--designs` synthetic designs resident in HBM,
+    timed with CUDA events on the call's stream, and training throughput (forward + backward +
+    Adam, minibatches of 64) on 4096 synthetic designs; both GEMM paths."""
+    import torch
+    import gdiamond_b200 as gd
+    from gdiamond_b200 import surrogate as S
+    dims, E, n = S.DIMS, 4, args.designs
+    flop_fwd = 2 * sum(a * b for a, b in zip(dims[:-1], dims[1:])) * E
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    pk = json.load(open(pk_path)) if os.path.exists(pk_path) else {"bf16_tflops": 1590.0}
+    peak, peak_kind = float(pk["bf16_tflops"]), "measured" if "hbm_gbs" in pk else "fallback"
+    x = torch.empty((n, dims[0]), device="cuda").uniform_(-1, 1)
+    mean = torch.empty((n, dims[-1]), device="cuda")
+    sd = torch.empty_like(mean)
+    rng = np.random.default_rng(0)
+    xs = rng.uniform(-1, 1, (4096, dims[0])).astype(np.float32)
+    ys = rng.normal(0, 1, (4096, dims[-1])).astype(np.float32)
+    out = {}
+    st = torch.cuda.current_stream()
+    for gemm in ("auto", "tcgen05", "mma_sync"):
+        net = gd.MLP(dims, members=E, seed=0, gemm=gemm)
+        for _ in range(args.warmup):
+            net.predict_device(x.data_ptr(), n, mean.data_ptr(), sd.data_ptr(), st)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            net.predict_device(x.data_ptr(), n, mean.data_ptr(), sd.data_ptr(), st)
+        e1.record(st)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3 / args.steps
+        net.set_data(xs, ys)
+        net.train(epochs=1, batch=64)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        net.train(epochs=args.train_epochs, batch=64)
+        t_train = time.perf_counter() - t0
+        out[gemm] = {"inference_designs_per_s": n / sec, "inference_ms": sec * 1e3,
+                     "inference_tflops": flop_fwd * n / sec / 1e12,
+                     "frac_of_bf16_peak": flop_fwd * n / sec / 1e12 / peak,
+                     "train_epochs_per_s": args.train_epochs / t_train,
+                     "train_designs_per_s": args.train_epochs * len(xs) / t_train}
+        net.close()
+    line = {"metric": "MLP ensemble inference TFLOP/s (BF16 tensor cores, FP32 accumulate)",
+            "workload": f"4-member ensemble {dims}, {n} designs per call; training minibatches "
+                        f"of 64 on 4096 designs",
+            "peak_bf16_tflops": peak, "peak_kind": peak_kind, "results": out,
+            "data": "synthetic"}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -659,10 +715,14 @@ def main():
     ap.add_argument("--zchunks", type=int, default=0, help="force z-chunks")
     ap.add_argument("--min-blocks", type=int, default=0, help="force the register cap")
     ap.add_argument("--workload", default="plain",
-                    choices=["plain", "mixed", "batched", "surrogate"],
+                    choices=["plain", "mixed", "batched", "surrogate", "mlp"],
                     help="plain: the benchmark line; mixed / batched: the precision and "
                          "batching configurations (separate JSON lines)")
     ap.add_argument("--sims", type=int, default=64, help="batched workload: simulations")
+    ap.add_argument("--batch-storage", default="bf16,f16,f32",
+                    help="batched workload: storages of the batched runs")
+    ap.add_argument("--designs", type=int, default=1 << 20, help="mlp: designs per inference")
+    ap.add_argument("--train-epochs", type=int, default=10, help="mlp: timed training epochs")
     ap.add_argument("--train", type=int, default=4096, help="surrogate: training designs")
     ap.add_argument("--test", type=int, default=512, help="surrogate: held-out designs")
     ap.add_argument("--epochs", type=int, default=200, help="surrogate: training epochs")
@@ -682,6 +742,8 @@ def main():
         return run_batched(args)
     if args.workload == "surrogate":
         return run_surrogate(args)
+    if args.workload == "mlp":
+        return run_mlp(args)
     return run_ours(args)
 
 

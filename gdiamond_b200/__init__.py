@@ -385,9 +385,9 @@ class MLP:
     [members][n_params]; ``layout()`` gives each layer's weight and bias offsets.
     """
 
-    GEMMS = {"tcgen05": 0, "mma_sync": 1}
+    GEMMS = {"tcgen05": 0, "mma_sync": 1, "auto": 2}
 
-    def __init__(self, dims, members=4, seed=0, device=0, gemm="tcgen05"):
+    def __init__(self, dims, members=4, seed=0, device=0, gemm="auto"):
         self.dims = tuple(int(d) for d in dims)
         self.members = int(members)
         self._L = library()
@@ -407,7 +407,8 @@ class MLP:
         self.set_gemm(gemm)
 
     def set_gemm(self, gemm):
-        """GEMM path: "tcgen05" (tensor-memory accumulator) or "mma_sync" (warp-level)."""
+        """GEMM path: "tcgen05" (tensor-memory accumulator), "mma_sync" (warp-level) or "auto"
+        (tcgen05 for products of >= 1024 rows, mma_sync for training minibatches)."""
         self._check(self._L.fdtd_mlp_set_gemm(self._h, self.GEMMS[gemm]))
         self.gemm = gemm
 

@@ -1078,12 +1078,23 @@ fdtd_status batch_launch(fdtd_batch* b, const fdtd::TiledConfig& c, int flip, lo
 fdtd_status batch_autotune(fdtd_batch* b, cudaStream_t st) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+  // A BLT or tile-row count that every simulation of the batch asks for (fdtd_desc) is kept;
+  // otherwise both are tuned.
+  int want_blt = b->sims[0]->desc.blt, want_rows = b->sims[0]->desc.tile_rows;
+  for (const fdtd_handle* h : b->sims) {
+    if (h->desc.blt != want_blt) want_blt = 0;
+    if (h->desc.tile_rows != want_rows) want_rows = 0;
+  }
   std::vector<fdtd::TiledConfig> cands;
   for (int rows : {16, 8})
     for (int blt = 1; blt <= 4; ++blt) {
+      if ((want_blt > 0 && blt != want_blt) || (want_rows > 0 && rows != want_rows)) continue;
       fdtd::TiledConfig c = batch_cfg(b, blt, rows);
       if (fdtd::tiled2_batch_supported(c)) cands.push_back(c);
     }
+  if (cands.empty())
+    return bfail(b, FDTD_ERR_UNSUPPORTED, "no batched configuration for blt %d, tile_rows %d",
+                 want_blt, want_rows);
   fdtd_status s = batch_counters(b, 4);
   if (s != FDTD_OK) return s;
   cudaEvent_t e0, e1;

@@ -9,9 +9,10 @@
 // feed a GEMM are BF16; every GEMM accumulates in FP32 on the tensor cores.  All members of the
 // ensemble run in the same launches (blockIdx.z = member), each on its own minibatch.
 //
-// Two GEMM paths compute the same products: tcgen05.mma with a TMEM accumulator (mlp_tc.cu, the
-// default) and the warp-level mma.sync.m16n8k16 kernel below (selectable with
-// fdtd_mlp_set_gemm; the cross-check of the first).
+// Two GEMM paths compute the same products: tcgen05.mma with a TMEM accumulator (mlp_tc.cu) and
+// the warp-level mma.sync.m16n8k16 kernel below.  The default (AUTO) runs products of >= 1024
+// rows (inference) on the first and the 64-row minibatch products of training on the second;
+// fdtd_mlp_set_gemm forces either (the tests cross-check them).
 //
 // GEMM: C[M][N] = sum_k opA(m,k) opB(n,k), opX(r,k) = TX ? X[k*ld + r] : X[r*ld + k], so one
 // kernel serves the forward pass (X W^T), the input gradient (G W) and the weight gradient
@@ -19,7 +20,8 @@
 // step's tile prefetched into registers, zero fill outside the matrices.  Fused epilogues:
 //   kStore      C = acc                                   (weight gradients)
 //   kBias       Z = acc + b                               (output layer)
-//   kBiasGelu   Z = acc + b, A = bf16(GELU(Z))            (hidden layers)
+//   kBiasGelu   Z = acc + b, A = bf16(GELU(Z))            (hidden layers, training)
+//   kBiasGeluAct A = bf16(GELU(acc + b))                  (hidden layers, inference)
 //   kGeluBack   G = acc * GELU'(Zp), Gbf = bf16(G)        (gradient through a hidden layer)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -293,7 +295,7 @@ struct fdtd_mlp {
   __nv_bfloat16* gbf[2] = {nullptr, nullptr};  // their BF16 copies
   float* tgt = nullptr;                        // [E][cap][out]
   float* xin = nullptr;                        // FP32 input staging [cap][in]
-  int gemm_kind = FDTD_MLP_GEMM_TCGEN05;
+  int gemm_kind = FDTD_MLP_GEMM_AUTO;
   mutable cudaError_t launch_err = cudaSuccess;  // first failed tcgen05 launch set-up
   int* d_err = nullptr;  // nonzero when a bounded wait in a GEMM kernel gave up
   std::string err;
@@ -360,7 +362,11 @@ Operand operand(const __nv_bfloat16* p, int ld, long long stride) {
 template <bool TA, bool TB, int EPI>
 void gemm(const fdtd_mlp* m, int M, int N, int K, const Operand& A, const Operand& B,
           const Epilogue& ep) {
-  if (m->gemm_kind == FDTD_MLP_GEMM_TCGEN05) {
+  // AUTO: the tensor-memory path for tall products; the warp-level kernel for the short
+  // minibatch products of training, where a 128-row tile would be half empty.
+  const bool tc = m->gemm_kind == FDTD_MLP_GEMM_TCGEN05 ||
+                  (m->gemm_kind == FDTD_MLP_GEMM_AUTO && M >= 1024);
+  if (tc) {
     const cudaError_t e =
         fdtd::mlp::launch_gemm_tc<TA, TB, EPI>(M, N, K, A, B, ep, m->E, m->st, m->d_err);
     if (e != cudaSuccess && m->launch_err == cudaSuccess) m->launch_err = e;
@@ -393,7 +399,7 @@ fdtd_status check_after(fdtd_mlp* m) {
 
 // Forward pass of every member on M rows of act[0] (member stride act0_stride; 0 when all
 // members see the same rows).  The output layer's result is z[L-1].
-void forward(fdtd_mlp* m, int M, long long act0_stride) {
+void forward(fdtd_mlp* m, int M, long long act0_stride, bool keep_z = true) {
   for (int l = 0; l < m->L; ++l) {
     const int in = m->dims[l], out = m->dims[l + 1];
     const long long sa = l == 0 ? act0_stride : m->cap * in;
@@ -407,7 +413,10 @@ void forward(fdtd_mlp* m, int M, long long act0_stride) {
     ep.stride_bias = m->P;
     if (l + 1 < m->L) {
       ep.out_bf = m->act[l + 1];
-      gemm<false, false, fdtd::mlp::kBiasGelu>(m, M, out, in, A, B, ep);
+      if (keep_z)
+        gemm<false, false, fdtd::mlp::kBiasGelu>(m, M, out, in, A, B, ep);
+      else
+        gemm<false, false, fdtd::mlp::kBiasGeluAct>(m, M, out, in, A, B, ep);
     } else {
       gemm<false, false, fdtd::mlp::kBias>(m, M, out, in, A, B, ep);
     }
@@ -481,7 +490,7 @@ fdtd_status predict_rows(fdtd_mlp* m, const float* x_dev, long long n, float* me
     const long long cnt = std::min<long long>(chunk, n - r0);
     fdtd::mlp::to_bf16<<<fdtd::mlp::nblocks(cnt * in), 256, 0, m->st>>>(cnt * in, x_dev + r0 * in,
                                                                          m->act[0]);
-    forward(m, (int)cnt, 0);
+    forward(m, (int)cnt, 0, /*keep_z=*/false);
     fdtd::mlp::ens_stats<<<fdtd::mlp::nblocks(cnt * out), 256, 0, m->st>>>(
         cnt * out, m->E, m->z[m->L - 1], m->cap * out, mean + r0 * out, sd + r0 * out);
     if (per_member)
@@ -561,7 +570,7 @@ fdtd_status fdtd_mlp_create(const int32_t* dims, int32_t n_dims, int32_t members
 }
 
 fdtd_status fdtd_mlp_set_gemm(fdtd_mlp* m, int32_t kind) {
-  if (!m || (kind != FDTD_MLP_GEMM_TCGEN05 && kind != FDTD_MLP_GEMM_MMA_SYNC))
+  if (!m || kind < FDTD_MLP_GEMM_TCGEN05 || kind > FDTD_MLP_GEMM_AUTO)
     return FDTD_ERR_INVALID_ARG;
   m->gemm_kind = kind;
   return FDTD_OK;

@@ -9,7 +9,7 @@
 namespace fdtd {
 namespace mlp {
 
-enum Epi { kStore = 0, kBias = 1, kBiasGelu = 2, kGeluBack = 3 };
+enum Epi { kStore = 0, kBias = 1, kBiasGelu = 2, kGeluBack = 3, kBiasGeluAct = 4 };
 
 // op(X)(r, k) = T ? X[k*ld + r] : X[r*ld + k] (+ member * stride)
 struct Operand {
@@ -21,8 +21,8 @@ struct Operand {
 
 struct Epilogue {
   float* out;              // C (kStore), Z (kBias, kBiasGelu), G (kGeluBack)
-  __nv_bfloat16* out_bf;   // A (kBiasGelu), Gbf (kGeluBack)
-  const float* bias;       // kBias, kBiasGelu
+  __nv_bfloat16* out_bf;   // A (kBiasGelu, kBiasGeluAct), Gbf (kGeluBack)
+  const float* bias;       // kBias, kBiasGelu, kBiasGeluAct
   const float* zp;         // kGeluBack: pre-activation of the layer below, same shape as out
   int ldc;
   long long stride_out, stride_bias, stride_zp;
@@ -41,15 +41,17 @@ __device__ __forceinline__ float gelu_grad(float z) {
 template <int EPI>
 __device__ __forceinline__ void epilogue_store(const Epilogue& ep, int e, int r, int c, float v) {
   const long long o = (long long)r * ep.ldc + c;
-  if (EPI == kBias || EPI == kBiasGelu) v += ep.bias[e * ep.stride_bias + c];
+  if (EPI == kBias || EPI == kBiasGelu || EPI == kBiasGeluAct) v += ep.bias[e * ep.stride_bias + c];
   if (EPI == kGeluBack) v *= gelu_grad(ep.zp[e * ep.stride_zp + o]);
-  ep.out[e * ep.stride_out + o] = v;
-  if (EPI == kBiasGelu) ep.out_bf[e * ep.stride_out + o] = __float2bfloat16_rn(gelu(v));
+  if (EPI != kBiasGeluAct) ep.out[e * ep.stride_out + o] = v;  // inference keeps no Z
+  if (EPI == kBiasGelu || EPI == kBiasGeluAct)
+    ep.out_bf[e * ep.stride_out + o] = __float2bfloat16_rn(gelu(v));
   if (EPI == kGeluBack) ep.out_bf[e * ep.stride_out + o] = __float2bfloat16_rn(v);
 }
 
 // tcgen05 GEMM (mlp_tc.cu): C[M][N] (+epilogue) for `members` members on `st`; `err` receives
-// a nonzero word if a bounded wait inside the kernel gave up.
+// a nonzero word if a bounded wait inside the kernel gave up.  Instantiated for the epilogues
+// the MLP uses (mlp_tc.cu lists them).
 template <bool TA, bool TB, int EPI>
 cudaError_t launch_gemm_tc(int M, int N, int K, const Operand& A, const Operand& B,
                            const Epilogue& ep, int members, cudaStream_t st, int* err);

@@ -3,17 +3,18 @@
 // C[M][N] = sum_k opA(m,k) opB(n,k) with BF16 operands and an FP32 accumulator held in tensor
 // memory, followed by the fused epilogues of mlp.cuh.  One CTA = 4 warps computes a 128 x BN
 // tile (BN = 64 or 128) for one ensemble member (blockIdx.z):
-//   - K advances in 64-wide steps through two shared-memory stages.  All 128 threads stage a
-//     step's A (128 x 64) and B (BN x 64) tiles from global memory, transposing where the
-//     operand is stored k-major, into the no-swizzle K-major "core matrix" layout the tensor
-//     core reads (8 rows x 16 bytes contiguous; the two 8-element halves of a K=16 slice 128 B
-//     apart, 8-row groups 1024 B apart).
+//   - K advances in 64-wide steps through two shared-memory stages.  All 128 threads load a
+//     step's A (128 x 64) and B (BN x 64) tiles from global memory into registers one step
+//     ahead, then write them, transposing where the operand is stored k-major, into the
+//     no-swizzle K-major "core matrix" layout the tensor core reads (8 rows x 16 bytes
+//     contiguous; the two 8-element halves of a K=16 slice 128 B apart, 8-row groups 1024 B
+//     apart).
 //   - One thread issues four tcgen05.mma (M=128, N=BN, K=16 each) per step and commits them to
 //     the stage's mbarrier; the next step's staging overlaps them, and a stage is refilled only
 //     after its commit arrives.
 //   - The accumulator (BN FP32 columns x 128 lanes) is allocated in TMEM by warp 0 and read back
-//     with tcgen05.ld (warp w owns lanes 32w..32w+31 = tile rows), 16 columns at a time, into
-//     the epilogue.
+//     with tcgen05.ld (warp w owns lanes 32w..32w+31 = tile rows), 32 columns at a time, and
+//     transposed through shared memory so the epilogue's stores are row-contiguous.
 // Every mbarrier wait is bounded; on expiry the kernel records an error word, stops issuing
 // (decided block-wide with __syncthreads_or), waits (bounded) for what it issued, skips the
 // epilogue, frees its TMEM and returns.
@@ -80,57 +81,87 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                    smem_u32(bar))
                : "memory");
 }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
       : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
         "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-        "=r"(v[14]), "=r"(v[15])
+        "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+        "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+        "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Stages rows [r0, r0+R) x k [k0, k0+64) of op(X) into the core-matrix tile at s (zeros outside
-// the R_tot x K matrix).
+// One thread's share of an R x 64 tile of op(X): R*8/128 chunks of 8 BF16 values.
+template <int R>
+struct Chunks {
+  uint4 v[R * 8 / 128];
+};
+
+// Chunk `it` of thread `tid`: (row, k) of its first element.  !T: 8 consecutive k of one row,
+// so a warp covers 4 whole core matrices (512 contiguous shared bytes).  T: 8 consecutive rows
+// at one k (contiguous in global memory).
 template <bool T, int R>
-__device__ __forceinline__ void stage_tile(uint8_t* s, const Operand& X, const __nv_bfloat16* base,
-                                           int R_tot, int K, int r0, int k0) {
-  const int tid = threadIdx.x;
+__device__ __forceinline__ void chunk_coords(int id, int* r, int* k) {
+  if (!T) {
+    *r = (id >> 6) * 8 + (id & 7);
+    *k = ((id >> 3) & 7) * 8;
+  } else {
+    *r = (id % (R / 8)) * 8;
+    *k = id / (R / 8);
+  }
+}
+
+// Loads rows [r0, r0+R) x k [k0, k0+64) of op(X) into registers (zeros outside R_tot x K).
+template <bool T, int R>
+__device__ __forceinline__ void load_tile(Chunks<R>& c, const Operand& X,
+                                          const __nv_bfloat16* base, int R_tot, int K, int r0,
+                                          int k0) {
   const __nv_bfloat16 zero = __float2bfloat16(0.0f);
 #pragma unroll
   for (int it = 0; it < R * 8 / 128; ++it) {
-    const int id = tid + it * 128;
+    int r, k;
+    chunk_coords<T, R>(threadIdx.x + it * 128, &r, &k);
+    const int gr = r0 + r, gk = k0 + k;
+    __nv_bfloat16 e[8];
     if (!T) {
-      // 8 consecutive k of one row; a warp writes 4 whole core matrices (512 contiguous bytes)
-      const int r = (id >> 6) * 8 + (id & 7), k = ((id >> 3) & 7) * 8;
-      const int gr = r0 + r, gk = k0 + k;
-      uint4 v;
       if (X.vec && gr < R_tot && gk + 8 <= K) {
-        v = *reinterpret_cast<const uint4*>(base + (long long)gr * X.ld + gk);
-      } else {
-        __nv_bfloat16 e[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          e[q] = (gr < R_tot && gk + q < K) ? base[(long long)gr * X.ld + gk + q] : zero;
-        memcpy(&v, e, 16);
+        c.v[it] = *reinterpret_cast<const uint4*>(base + (long long)gr * X.ld + gk);
+        continue;
       }
-      *reinterpret_cast<uint4*>(s + cm_off(r, k)) = v;
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        e[q] = (gr < R_tot && gk + q < K) ? base[(long long)gr * X.ld + gk + q] : zero;
     } else {
-      // 8 consecutive rows at one k (contiguous in memory), scattered to 8 rows of the tile
-      const int r = (id % (R / 8)) * 8, k = id / (R / 8);
-      const int gr = r0 + r, gk = k0 + k;
-      __nv_bfloat16 e[8];
       if (X.vec && gk < K && gr + 8 <= R_tot) {
-        const uint4 v = *reinterpret_cast<const uint4*>(base + (long long)gk * X.ld + gr);
-        memcpy(e, &v, 16);
-      } else {
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          e[q] = (gk < K && gr + q < R_tot) ? base[(long long)gk * X.ld + gr + q] : zero;
+        c.v[it] = *reinterpret_cast<const uint4*>(base + (long long)gk * X.ld + gr);
+        continue;
       }
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        e[q] = (gk < K && gr + q < R_tot) ? base[(long long)gk * X.ld + gr + q] : zero;
+    }
+    memcpy(&c.v[it], e, 16);
+  }
+}
+
+// Writes the registers of load_tile into the core-matrix tile at s.
+template <bool T, int R>
+__device__ __forceinline__ void store_tile(uint8_t* s, const Chunks<R>& c) {
+#pragma unroll
+  for (int it = 0; it < R * 8 / 128; ++it) {
+    int r, k;
+    chunk_coords<T, R>(threadIdx.x + it * 128, &r, &k);
+    if (!T) {
+      *reinterpret_cast<uint4*>(s + cm_off(r, k)) = c.v[it];
+    } else {
+      __nv_bfloat16 e[8];
+      memcpy(e, &c.v[it], 16);
 #pragma unroll
       for (int q = 0; q < 8; ++q) *reinterpret_cast<__nv_bfloat16*>(s + cm_off(r + q, k)) = e[q];
     }
@@ -181,6 +212,10 @@ __global__ void __launch_bounds__(128) gemm_tc(int M, int N, int K, Operand A, O
   const int nk = (K + TBK - 1) / TBK;
   int issued = 0;  // K steps whose MMAs were issued and committed
   bool aborted = false;
+  Chunks<TBM> ca;
+  Chunks<BN> cb;
+  load_tile<TA, TBM>(ca, A, Ab, M, K, m0, 0);
+  load_tile<TB, BN>(cb, B, Bb, N, K, n0, 0);
   for (int kt = 0; kt < nk; ++kt) {
     const int s = kt & 1;
     bool bad = false;
@@ -189,13 +224,17 @@ __global__ void __launch_bounds__(128) gemm_tc(int M, int N, int K, Operand A, O
       atomicExch(err, 1);
     }
     if (!bad) {
-      stage_tile<TA, TBM>(sA + s * L::A_BYTES, A, Ab, M, K, m0, kt * TBK);
-      stage_tile<TB, BN>(sB + s * L::B_BYTES, B, Bb, N, K, n0, kt * TBK);
+      store_tile<TA, TBM>(sA + s * L::A_BYTES, ca);
+      store_tile<TB, BN>(sB + s * L::B_BYTES, cb);
     }
     fence_proxy_async_smem();
     if (__syncthreads_or(bad)) {  // a barrier whose result every thread shares
       aborted = true;
       break;
+    }
+    if (kt + 1 < nk) {  // the next step's loads fly while this step's MMAs are issued
+      load_tile<TA, TBM>(ca, A, Ab, M, K, m0, (kt + 1) * TBK);
+      load_tile<TB, BN>(cb, B, Bb, N, K, n0, (kt + 1) * TBK);
     }
     if (tid == 0) {
       tc_fence_after();
@@ -218,19 +257,25 @@ __global__ void __launch_bounds__(128) gemm_tc(int M, int N, int K, Operand A, O
   late = __syncthreads_or(late);
   tc_fence_after();
   if (!late && !aborted && issued > 0) {
-    const int row = m0 + warp * 32 + lane;
+    // Warp w holds rows 32w..32w+31 of the tile in its TMEM lanes.  Each 32-column block goes
+    // through a padded 32 x 33 shared buffer (the drained A stage) so that every store
+    // instruction writes 32 consecutive columns of one row.
+    float* buf = reinterpret_cast<float*>(sA) + warp * (32 * 33);
 #pragma unroll 1
-    for (int c0 = 0; c0 < BN && n0 + c0 < N; c0 += 16) {
-      uint32_t v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+    for (int c0 = 0; c0 < BN && n0 + c0 < N; c0 += 32) {
+      uint32_t v[32];
+      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
       tmem_wait_ld();
-      if (row < M) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int c = n0 + c0 + q;
-          if (c < N) epilogue_store<EPI>(ep, e, row, c, __uint_as_float(v[q]));
-        }
+      for (int j = 0; j < 32; ++j) buf[lane * 33 + j] = __uint_as_float(v[j]);
+      __syncwarp();
+      const int c = n0 + c0 + lane;
+#pragma unroll 4
+      for (int rr = 0; rr < 32; ++rr) {
+        const int row = m0 + warp * 32 + rr;
+        if (row < M && c < N) epilogue_store<EPI>(ep, e, row, c, buf[rr * 33 + lane]);
       }
+      __syncwarp();
     }
   }
   tc_fence_before();
@@ -267,10 +312,14 @@ cudaError_t launch_gemm_tc(int M, int N, int K, const Operand& A, const Operand&
   return launch_bn<TA, TB, EPI, 128>(M, N, K, A, B, ep, members, st, err);
 }
 
-// The instances the MLP uses: forward (X W^T), weight gradient (G^T X), input gradient (G W).
+// The instances the MLP uses: forward (X W^T; training keeps Z, inference only the BF16
+// activation), weight gradient (G^T X), input gradient (G W).
 template cudaError_t launch_gemm_tc<false, false, kBiasGelu>(int, int, int, const Operand&,
                                                              const Operand&, const Epilogue&, int,
                                                              cudaStream_t, int*);
+template cudaError_t launch_gemm_tc<false, false, kBiasGeluAct>(int, int, int, const Operand&,
+                                                                const Operand&, const Epilogue&,
+                                                                int, cudaStream_t, int*);
 template cudaError_t launch_gemm_tc<false, false, kBias>(int, int, int, const Operand&,
                                                          const Operand&, const Epilogue&, int,
                                                          cudaStream_t, int*);

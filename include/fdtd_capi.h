@@ -232,11 +232,13 @@ const char* fdtd_batch_last_error(const fdtd_batch* b);
  * of 8 floats; gaps are zero).  get/set_params move all members: [members][n_params]. */
 typedef struct fdtd_mlp fdtd_mlp;
 
-/* GEMM path of an ensemble: tcgen05.mma with the accumulator in tensor memory (default), or the
- * warp-level mma.sync kernel (the same products; kept as a cross-check). */
+/* GEMM path of an ensemble: tcgen05.mma with the accumulator in tensor memory, the warp-level
+ * mma.sync kernel (the same products), or AUTO (default): tcgen05 for products of >= 1024
+ * rows (inference), mma.sync for the short minibatch products of training. */
 typedef enum fdtd_mlp_gemm {
   FDTD_MLP_GEMM_TCGEN05 = 0,
-  FDTD_MLP_GEMM_MMA_SYNC = 1
+  FDTD_MLP_GEMM_MMA_SYNC = 1,
+  FDTD_MLP_GEMM_AUTO = 2
 } fdtd_mlp_gemm;
 
 fdtd_status fdtd_mlp_create(const int32_t* dims, int32_t n_dims, int32_t members, uint64_t seed,
