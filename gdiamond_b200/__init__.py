@@ -39,7 +39,8 @@ EXPORTS = (
     "fdtd_mlp_create", "fdtd_mlp_destroy", "fdtd_mlp_last_error", "fdtd_mlp_layout",
     "fdtd_mlp_get_params", "fdtd_mlp_set_params", "fdtd_mlp_set_data", "fdtd_mlp_grad",
     "fdtd_mlp_train", "fdtd_mlp_predict", "fdtd_mlp_predict_device", "fdtd_get_dft_device",
-    "fdtd_mlp_set_gemm",
+    "fdtd_mlp_set_gemm", "fdtd_get_planes_device", "fdtd_set_planes_device",
+    "fdtd_storage_bytes",
 )
 
 
@@ -96,6 +97,9 @@ def library():
             "fdtd_get_config": ([V, P(C.c_int32)], C.c_int),
             "fdtd_get_field_f64": ([V, C.c_int32, P(C.c_double)], C.c_int),
             "fdtd_get_dft_device": ([V, C.c_int32, V, V, V], C.c_int),
+            "fdtd_get_planes_device": ([V, C.c_int32, C.c_int64, C.c_int64, V, V], C.c_int),
+            "fdtd_set_planes_device": ([V, C.c_int32, C.c_int64, C.c_int64, V, V], C.c_int),
+            "fdtd_storage_bytes": ([V, P(C.c_int32)], C.c_int),
             "fdtd_batch_create": ([P(V), C.c_int32, P(V)], C.c_int),
             "fdtd_batch_destroy": ([V], C.c_int),
             "fdtd_batch_step": ([V, C.c_int64, C.c_int32, V], C.c_int),
@@ -130,6 +134,13 @@ def library():
 
 def _fp(a, T=C.c_float):
     return a.ctypes.data_as(C.POINTER(T))
+
+
+def _stream(stream):
+    """A torch.cuda.Stream, an int handle or None as a cudaStream_t argument."""
+    if stream is None:
+        return None
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
 
 
 class Simulation:
@@ -321,6 +332,23 @@ class Simulation:
         self._check(self._L.fdtd_get_dft(self._h, monitor_id, _fp(re, C.c_double),
                                           _fp(im, C.c_double)))
         return re, im
+
+    def storage_bytes(self):
+        n = C.c_int32()
+        self._check(self._L.fdtd_storage_bytes(self._h, C.byref(n)))
+        return n.value
+
+    def get_planes_device(self, component, k0, nk, ptr, stream=None):
+        """Raw copy of z-planes [k0, k0+nk) of a component (current set) to a device buffer."""
+        comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
+        self._check(self._L.fdtd_get_planes_device(self._h, comp, int(k0), int(nk),
+                                                    C.c_void_p(ptr), _stream(stream)))
+
+    def set_planes_device(self, component, k0, nk, ptr, stream=None):
+        """Raw copy of a device buffer into z-planes [k0, k0+nk) of a component (current set)."""
+        comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
+        self._check(self._L.fdtd_set_planes_device(self._h, comp, int(k0), int(nk),
+                                                    C.c_void_p(ptr), _stream(stream)))
 
     def get_dft_device(self, monitor_id, re_ptr, im_ptr, stream=None):
         """Copy a monitor's running sums into device arrays (float64 [nf][ny][nx] pointers)."""

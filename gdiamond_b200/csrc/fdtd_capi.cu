@@ -909,6 +909,42 @@ fdtd_status fdtd_get_dft_device(fdtd_handle* h, int32_t monitor_id, double* re_d
   return FDTD_OK;
 }
 
+// Raw (storage-format) copies of z-planes [k0, k0+nk) of one component of the current field
+// set: the halo exchange of z-slab decomposition.
+fdtd_status plane_copy(fdtd_handle* h, int32_t comp, int64_t k0, int64_t nk, void* dev,
+                       void* stream, bool to_handle) {
+  if (!h || !dev || comp < 0 || comp > 5 || k0 < 0 || nk < 1 || k0 + nk > h->g.nz)
+    return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  cudaStream_t st = pick_stream(h, stream);
+  const size_t esz = (size_t)h->esz;
+  char* field = reinterpret_cast<char*>(h->F[h->cur][comp]) + (size_t)k0 * h->g.plane * esz;
+  char* packed = static_cast<char*>(dev);
+  const size_t row = (size_t)h->g.nx * esz, pitch = (size_t)h->g.pitch * esz;
+  const size_t rows = (size_t)h->g.ny * (size_t)nk;
+  if (to_handle)
+    CUDA_TRY(h, cudaMemcpy2DAsync(field, pitch, packed, row, row, rows, cudaMemcpyDeviceToDevice, st));
+  else
+    CUDA_TRY(h, cudaMemcpy2DAsync(packed, row, field, pitch, row, rows, cudaMemcpyDeviceToDevice, st));
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_get_planes_device(fdtd_handle* h, int32_t component, int64_t k0, int64_t nk,
+                                   void* dev_out, void* stream) {
+  return plane_copy(h, component, k0, nk, dev_out, stream, false);
+}
+
+fdtd_status fdtd_set_planes_device(fdtd_handle* h, int32_t component, int64_t k0, int64_t nk,
+                                   const void* dev_in, void* stream) {
+  return plane_copy(h, component, k0, nk, const_cast<void*>(dev_in), stream, true);
+}
+
+fdtd_status fdtd_storage_bytes(const fdtd_handle* h, int32_t* esz) {
+  if (!h || !esz) return FDTD_ERR_INVALID_ARG;
+  *esz = h->esz;
+  return FDTD_OK;
+}
+
 fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6) {
   if (!h || !scale6) return FDTD_ERR_INVALID_ARG;
   for (int c = 0; c < 6; ++c)

@@ -165,6 +165,16 @@ fdtd_status fdtd_get_dft(fdtd_handle* h, int32_t monitor_id, double* re, double*
  * counterpart: gDiamond reads its DFT sums on the host only. */
 fdtd_status fdtd_get_dft_device(fdtd_handle* h, int32_t monitor_id, double* re_dev,
                                 double* im_dev, void* stream);
+/* Raw copies of the z-planes [k0, k0+nk) of one component of the current field set between the
+ * handle and an unpitched device buffer of nk*Ny*Nx values in the storage format (esz bytes
+ * each, fdtd_storage_bytes), on `stream` (NULL: the handle's stream; asynchronous).  The halo
+ * exchange of a grid split into z-slabs (gdiamond_b200/slabs.py).  No reference counterpart:
+ * gDiamond runs one grid on one GPU. */
+fdtd_status fdtd_get_planes_device(fdtd_handle* h, int32_t component, int64_t k0, int64_t nk,
+                                   void* dev_out, void* stream);
+fdtd_status fdtd_set_planes_device(fdtd_handle* h, int32_t component, int64_t k0, int64_t nk,
+                                   const void* dev_in, void* stream);
+fdtd_status fdtd_storage_bytes(const fdtd_handle* h, int32_t* esz);
 /* Device-to-device field copy into an unpitched Nx*Ny*Nz float array (asynchronous). */
 fdtd_status fdtd_get_field_device(fdtd_handle* h, int32_t component, float* dev_out,
                                   void* stream);
