@@ -247,3 +247,84 @@ def exchange_dist(plan, rank, get_block, put_block, make_buffer):
         q.wait()
     for k0, nk, buf in recvs:
         put_block(k0, nk, buf)
+
+
+class DistZSlab:
+    """This process's part of a grid split over the ranks of the default torch.distributed group
+    (one rank per GPU; NCCL moves the halo planes over NVLink between device buffers).
+
+    Every rank constructs it with the same global arguments and calls the same methods in the
+    same order; step(T) runs blocks of `halo` steps, each followed by exchange_dist().
+    """
+
+    def __init__(self, nx, ny, nz, halo=2, device=None, storage="f32", tile_rows=0,
+                 kernel="tiled"):
+        import torch
+        import torch.distributed as dist
+        self.rank, self.world = dist.get_rank(), dist.get_world_size()
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self.shape = (int(nx), int(ny), int(nz))
+        self.plan = HaloPlan(nz, self.world, halo)
+        self.lo = self.plan.loc[self.rank][0]
+        self.sim = Simulation(nx, ny, self.plan.local_nz(self.rank), device=self.device,
+                              kernel=kernel, blt=halo, tile_rows=tile_rows, storage=storage)
+        self.esz = self.sim.storage_bytes()
+        self.monitors = []
+        self.t = 0
+
+    def set_coefficients(self, coef12):
+        lo, hi = self.plan.loc[self.rank]
+        self.sim.set_coefficients([slice_planes(c, self.shape, lo, hi) for c in coef12])
+
+    def set_sources(self, sources):
+        self.sim.set_sources(localize_sources(self.plan, self.rank, list(sources)))
+
+    def add_dft_monitor(self, component, k, freqs, scale=1.0, dt=np.float32(0.05)):
+        """Registers the monitor on its owner; returns (owner rank, id on the owner)."""
+        r = self.plan.owner(int(k))
+        mid = None
+        if r == self.rank:
+            mid = self.sim.add_dft_monitor(component, self.plan.to_local(r, int(k)), freqs,
+                                           scale, dt)
+        self.monitors.append((r, mid))
+        return len(self.monitors) - 1
+
+    def exchange(self):
+        import torch
+        nx, ny, _ = self.shape
+        dev = f"cuda:{self.device}"
+        stream = torch.cuda.current_stream(self.device)
+
+        def get_block(k0, nk):
+            return _block(self.sim, k0 - self.lo, nk, self.esz, dev, stream)
+
+        def put_block(k0, nk, buf):
+            _unblock(self.sim, k0 - self.lo, nk, buf, stream)
+
+        def make_buffer(nk):
+            return torch.empty((6, nk, ny, nx), dtype=getattr(torch, _RAW[self.esz]), device=dev)
+
+        exchange_dist(self.plan, self.rank, get_block, put_block, make_buffer)
+
+    def step(self, T, stream=None):
+        """T steps on the current torch stream (the halo copies and NCCL run on it too)."""
+        import torch
+        st = torch.cuda.current_stream(self.device) if stream is None else stream
+        done = 0
+        while done < int(T):
+            b = min(self.plan.halo, int(T) - done)
+            self.sim.step(b, st)
+            if self.world > 1:
+                self.exchange()
+            done += b
+        self.t += int(T)
+
+    def owned_field(self, component):
+        """This rank's owned planes of a component ([planes][ny][nx] float32)."""
+        nx, ny, _ = self.shape
+        lo, hi = self.plan.own[self.rank]
+        f = self.sim.get_field(component).reshape(-1, ny, nx)
+        return f[lo - self.lo:hi - self.lo]
+
+    def close(self):
+        self.sim.close()
