@@ -40,7 +40,7 @@ EXPORTS = (
     "fdtd_mlp_get_params", "fdtd_mlp_set_params", "fdtd_mlp_set_data", "fdtd_mlp_grad",
     "fdtd_mlp_train", "fdtd_mlp_predict", "fdtd_mlp_predict_device", "fdtd_get_dft_device",
     "fdtd_mlp_set_gemm", "fdtd_get_planes_device", "fdtd_set_planes_device",
-    "fdtd_storage_bytes",
+    "fdtd_storage_bytes", "fdtd_set_step", "fdtd_set_dft",
 )
 
 
@@ -100,6 +100,8 @@ def library():
             "fdtd_get_planes_device": ([V, C.c_int32, C.c_int64, C.c_int64, V, V], C.c_int),
             "fdtd_set_planes_device": ([V, C.c_int32, C.c_int64, C.c_int64, V, V], C.c_int),
             "fdtd_storage_bytes": ([V, P(C.c_int32)], C.c_int),
+            "fdtd_set_step": ([V, C.c_int64], C.c_int),
+            "fdtd_set_dft": ([V, C.c_int32, P(C.c_double), P(C.c_double)], C.c_int),
             "fdtd_batch_create": ([P(V), C.c_int32, P(V)], C.c_int),
             "fdtd_batch_destroy": ([V], C.c_int),
             "fdtd_batch_step": ([V, C.c_int64, C.c_int32, V], C.c_int),
@@ -162,6 +164,7 @@ class Simulation:
         if st != 0:
             raise FdtdError(st, self._L.fdtd_last_error(None).decode())
         self._h = h
+        self._device = int(device)
         self._keep = []
         self.n_monitors = 0
         self._monitor_nf = []
@@ -349,6 +352,50 @@ class Simulation:
         comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
         self._check(self._L.fdtd_set_planes_device(self._h, comp, int(k0), int(nk),
                                                     C.c_void_p(ptr), _stream(stream)))
+
+    def set_dft(self, monitor_id, re, im):
+        re = np.ascontiguousarray(re, np.float64)
+        im = np.ascontiguousarray(im, np.float64)
+        nx, ny, _ = self.shape
+        if re.size != self._monitor_nf[monitor_id] * nx * ny or im.size != re.size:
+            raise ValueError("DFT sums of the wrong size")
+        self._check(self._L.fdtd_set_dft(self._h, int(monitor_id), _fp(re, C.c_double),
+                                          _fp(im, C.c_double)))
+
+    def checkpoint(self):
+        """The whole state as host arrays: step counter, the current field set in its storage
+        format (raw), every monitor's sums.  restore() on a handle with the same shape,
+        storage, sources and monitors continues bit for bit."""
+        import torch
+        self.sync()
+        nx, ny, nz = self.shape
+        esz = self.storage_bytes()
+        raw = {2: torch.int16, 4: torch.int32, 8: torch.int64}[esz]
+        dev = torch.device("cuda", self._device)
+        buf = torch.empty((nz, ny, nx), dtype=raw, device=dev)
+        fields = []
+        for c in range(6):
+            self.get_planes_device(c, 0, nz, buf.data_ptr())
+            self.sync()
+            fields.append(buf.cpu().numpy().copy())
+        return {"t": self.t, "shape": self.shape, "esz": esz, "fields": fields,
+                "dft": [self.get_dft(m) for m in range(self.n_monitors)]}
+
+    def restore(self, ckpt):
+        import torch
+        if tuple(ckpt["shape"]) != self.shape or ckpt["esz"] != self.storage_bytes():
+            raise ValueError("checkpoint of another shape or storage")
+        if len(ckpt["dft"]) != self.n_monitors:
+            raise ValueError("checkpoint with another set of monitors")
+        nz = self.shape[2]
+        self.sync()
+        for c, f in enumerate(ckpt["fields"]):
+            t = torch.from_numpy(np.ascontiguousarray(f)).to(torch.device("cuda", self._device))
+            self.set_planes_device(c, 0, nz, t.data_ptr())
+            self.sync()
+        for m, (re, im) in enumerate(ckpt["dft"]):
+            self.set_dft(m, re, im)
+        self._check(self._L.fdtd_set_step(self._h, int(ckpt["t"])))
 
     def get_dft_device(self, monitor_id, re_ptr, im_ptr, stream=None):
         """Copy a monitor's running sums into device arrays (float64 [nf][ny][nx] pointers)."""

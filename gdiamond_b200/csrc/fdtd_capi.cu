@@ -802,6 +802,25 @@ fdtd_status fdtd_sync(fdtd_handle* h) {
   return check_device_error(h);
 }
 
+fdtd_status fdtd_set_step(fdtd_handle* h, int64_t t) {
+  if (!h || t < 0) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  h->t = t;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_set_dft(fdtd_handle* h, int32_t monitor_id, const double* re, const double* im) {
+  if (!h || monitor_id < 0 || monitor_id >= h->nmon || !re || !im) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  const MonitorHost& m = h->mon[monitor_id];
+  const size_t bytes = (size_t)m.nf * h->g.nx * h->g.ny * sizeof(double);
+  CUDA_TRY(h, cudaMemcpyAsync(m.re, re, bytes, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(m.im, im, bytes, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return FDTD_OK;
+}
+
 fdtd_status fdtd_get_step(const fdtd_handle* h, int64_t* t) {
   if (!h || !t) return FDTD_ERR_INVALID_ARG;
   *t = h->t;

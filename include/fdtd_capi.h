@@ -160,6 +160,12 @@ fdtd_status fdtd_get_step(const fdtd_handle* h, int64_t* t);
 fdtd_status fdtd_get_field(fdtd_handle* h, int32_t component, float* host_out);
 fdtd_status fdtd_set_field(fdtd_handle* h, int32_t component, const float* host_in);
 fdtd_status fdtd_get_dft(fdtd_handle* h, int32_t monitor_id, double* re, double* im);
+/* Checkpoint / resume (no reference counterpart: gDiamond restarts every run from zero).  With
+ * the raw field planes (fdtd_get/set_planes_device) these restore a handle's whole state: the
+ * step counter (which indexes the source waveforms and the DFT phase) and a monitor's sums
+ * ([nf][Ny][Nx] doubles each, host buffers). */
+fdtd_status fdtd_set_step(fdtd_handle* h, int64_t t);
+fdtd_status fdtd_set_dft(fdtd_handle* h, int32_t monitor_id, const double* re, const double* im);
 /* Device-to-device copy of a monitor's running sums into [nf][Ny][Nx] double arrays on
  * `stream` (a cudaStream_t or NULL for the handle's stream; asynchronous).  No reference
  * counterpart: gDiamond reads its DFT sums on the host only. */

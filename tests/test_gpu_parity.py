@@ -285,3 +285,47 @@ def test_gpu_coefficient_builder_matches_reference_formula(shape):
         assert sim.material_count() == sim2.material_count() > 1
         sim.close()
         sim2.close()
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+def test_checkpoint_resume_continues_bit_for_bit(storage):
+    """checkpoint() after 13 steps, restore() into a fresh handle, 11 more steps: the same
+    fields and DFT sums as 24 uninterrupted steps.  16-bit storage rounds once per BLT-step
+    pass, so there the split falls on a pass boundary (12 + 12: a multiple of every BLT the
+    16-bit kernel uses); FP32 / FP64 split anywhere."""
+    first = 12 if storage == "f16" else 13
+    shape = (45, 33, 27)
+    eps = W.spheres_eps(shape, n_spheres=3, r_range=(3, 6), seed=5)
+    coefs = W.reference_coefficients(shape, eps_re=eps)
+    w = W.gaussian_wave(24, delay=6.0, width=2.5, period=5.0)
+    src = [dict(component="Jy", wave=w, i=20, j=15, k=12)]
+    freqs = W.source_band(3, period=5.0, width=2.5)
+
+    def make():
+        sim = gd.Simulation(*shape, storage=storage)
+        if storage == "f16":
+            sim.set_storage_scale([4.0] * 3 + [1.0] * 3)
+        sim.set_coefficients(coefs)
+        sim.set_sources(src)
+        sim.add_dft_monitor("Ey", 14, freqs)
+        return sim
+
+    a = make()
+    a.step(24)
+    a.sync()
+    want = a.checkpoint()
+    b = make()
+    b.step(first)
+    ck = b.checkpoint()
+    b.close()
+    c = make()
+    c.restore(ck)
+    assert c.t == first
+    c.step(24 - first)
+    got = c.checkpoint()
+    for f, g in zip(got["fields"], want["fields"]):
+        assert np.array_equal(f, g)
+    assert np.abs(want["dft"][0][0]).max() > 0
+    assert all(np.array_equal(x, y) for x, y in zip(got["dft"][0], want["dft"][0]))
+    a.close()
+    c.close()
