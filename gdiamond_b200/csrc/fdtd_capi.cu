@@ -266,7 +266,7 @@ fdtd::TiledArgs make_tiled_args(fdtd_handle* h, const fdtd::TiledConfig& c, long
 // Candidate tiled configurations for the autotuner.
 std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
   std::vector<fdtd::TiledConfig> out;
-  std::vector<int> blts = {1, 2, 3, 4, 5, 6}, rows_l = {8, 16, 32}, zc = {1, 2, 4, 8};
+  std::vector<int> blts = {1, 2, 3, 4, 5, 6}, rows_l = {8, 16, 20, 24, 32}, zc = {1, 2, 4, 8};
   std::vector<int> widths = {32, 64};
   const bool half = h->esz == 2;
   if (half) {
@@ -507,8 +507,9 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
       d->kernel != FDTD_KERNEL_NAIVE)
     return fail(nullptr, FDTD_ERR_UNSUPPORTED, "FP64 field storage runs the naive kernel only");
   if (d->blt < 0 || d->blt > 6) return fail(nullptr, FDTD_ERR_INVALID_ARG, "blt must be 0..6");
-  if (d->tile_rows != 0 && d->tile_rows != 8 && d->tile_rows != 16 && d->tile_rows != 32)
-    return fail(nullptr, FDTD_ERR_INVALID_ARG, "tile_rows must be 0, 8, 16 or 32");
+  if (d->tile_rows != 0 && d->tile_rows != 8 && d->tile_rows != 16 && d->tile_rows != 20 &&
+      d->tile_rows != 24 && d->tile_rows != 32)
+    return fail(nullptr, FDTD_ERR_INVALID_ARG, "tile_rows must be 0, 8, 16, 20, 24 or 32");
   if (d->z_chunks < 0) return fail(nullptr, FDTD_ERR_INVALID_ARG, "z_chunks must be >= 0");
   if (d->min_blocks != 0 && d->min_blocks != 1 && d->min_blocks != 2 && d->min_blocks != 4)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "min_blocks must be 0, 1, 2 or 4");
@@ -1141,7 +1142,7 @@ fdtd_status batch_autotune(fdtd_batch* b, cudaStream_t st) {
     if (h->desc.tile_rows != want_rows) want_rows = 0;
   }
   std::vector<fdtd::TiledConfig> cands;
-  for (int rows : {16, 8})
+  for (int rows : {16, 8, 20, 24})
     for (int blt = 1; blt <= 4; ++blt) {
       if ((want_blt > 0 && blt != want_blt) || (want_rows > 0 && rows != want_rows)) continue;
       fdtd::TiledConfig c = batch_cfg(b, blt, rows);

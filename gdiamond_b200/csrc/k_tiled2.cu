@@ -83,13 +83,14 @@ struct Tiled2 {
   static constexpr int W = 64;                 // cells per warp row
   static constexpr int PL = W * TY;            // elements of one staged field plane
   static constexpr int MPL = kMatBoxX2 * TY;   // elements of one staged material plane
+  static constexpr int MPL_S = (MPL * 2 + 127) / 128 * 64;  // its stage stride: 128-byte steps
   static constexpr int NS = ESZ == 4 ? kTiled2Stages : kTiled2Stages + 1;
   static constexpr int SX = tiled2_sx(B, ESZ);
   static constexpr int SY = tiled_sy(B, TY);
   static constexpr int XBASE = tiled2_xbase(B, ESZ);
   static constexpr uint32_t STAGE_F_BYTES = 6u * PL * ESZ;
-  static constexpr uint32_t STAGE_M_BYTES = MPL * 2u;
-  static constexpr uint32_t TX_BYTES = STAGE_F_BYTES + STAGE_M_BYTES;
+  static constexpr uint32_t STAGE_M_BYTES = MPL_S * 2u;  // TMA destinations stay 128-aligned
+  static constexpr uint32_t TX_BYTES = STAGE_F_BYTES + MPL * 2u;  // bytes the copies deliver
   static constexpr size_t OFF_M = (size_t)NS * STAGE_F_BYTES;
   static constexpr size_t OFF_H = OFF_M + (size_t)NS * STAGE_M_BYTES;
   static constexpr size_t OFF_E = OFF_H + 2u * 2u * PL * 4u;
@@ -192,7 +193,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     const int pz = ps + it_;
 #pragma unroll
     for (int c = 0; c < 6; ++c) tma_load_3d(d + c * K::PL, &a.tm_src[c], bar, X, Y, pz);
-    tma_load_3d(st_m + stage * K::MPL, &a.tm_mat, bar, X8, Y, pz);
+    tma_load_3d(st_m + stage * K::MPL_S, &a.tm_mat, bar, X8, Y, pz);
   };
   if (tid == 0) {
     fence_proxy_async_smem();
@@ -234,7 +235,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     const S* S0 = st_f + stage * 6 * K::PL;
 #pragma unroll
     for (int s = B; s >= 1; --s) mq[s] = mq[s - 1];
-    mq[0] = *reinterpret_cast<const uint32_t*>(st_m + stage * K::MPL + om);
+    mq[0] = *reinterpret_cast<const uint32_t*>(st_m + stage * K::MPL_S + om);
     Pair Hc[3], Eo[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -510,7 +511,7 @@ cudaError_t launch_rows2(int blt, int min_blocks, const TiledArgs& a, dim3 grid,
   switch (blt) {
     case 1: return launch_one2<S, 1, TY, 1>(a, grid, st);
     case 2: return launch_one2<S, 2, TY, 1>(a, grid, st);
-    case 3: if constexpr (TY < 32) return launch_one2<S, 3, TY, 1>(a, grid, st); break;
+    case 3: if constexpr (TY <= 20) return launch_one2<S, 3, TY, 1>(a, grid, st); break;
     case 4: if constexpr (TY == 16) return launch_one2<S, 4, TY, 1>(a, grid, st); break;
     default: break;
   }
@@ -522,6 +523,12 @@ cudaError_t launch_type2(const TiledConfig& c, const TiledArgs& a, dim3 grid, cu
   switch (c.rows) {
     case 8: return launch_rows2<S, 8>(c.blt, c.min_blocks, a, grid, st);
     case 16: return launch_rows2<S, 16>(c.blt, c.min_blocks, a, grid, st);
+    case 20:  // FP32: 640 threads, the register file's limit at ~96 registers per thread
+      if constexpr (sizeof(S) == 4) return launch_rows2<S, 20>(c.blt, c.min_blocks, a, grid, st);
+      break;
+    case 24:
+      if constexpr (sizeof(S) == 4) return launch_rows2<S, 24>(c.blt, c.min_blocks, a, grid, st);
+      break;
     case 32:
       if constexpr (sizeof(S) == 4) return launch_rows2<S, 32>(c.blt, c.min_blocks, a, grid, st);
       break;
@@ -547,6 +554,21 @@ cudaError_t launch_batch_type(const TiledConfig& c, const BatchArgs& b, int ctas
       case 2: return launch_batch_one<S, 2, 8>(b, ctas, st);
       case 3: return launch_batch_one<S, 3, 8>(b, ctas, st);
       default: break;
+    }
+  } else if constexpr (sizeof(S) == 4) {
+    if (c.rows == 20) {
+      switch (c.blt) {
+        case 1: return launch_batch_one<S, 1, 20>(b, ctas, st);
+        case 2: return launch_batch_one<S, 2, 20>(b, ctas, st);
+        case 3: return launch_batch_one<S, 3, 20>(b, ctas, st);
+        default: break;
+      }
+    } else if (c.rows == 24) {
+      switch (c.blt) {
+        case 1: return launch_batch_one<S, 1, 24>(b, ctas, st);
+        case 2: return launch_batch_one<S, 2, 24>(b, ctas, st);
+        default: break;
+      }
     }
   }
   return cudaErrorInvalidValue;
@@ -583,6 +605,19 @@ int batch_occupancy_type(const TiledConfig& c) {
       case 2: return occupancy_of<S, 2, 8>();
       case 3: return occupancy_of<S, 3, 8>();
     }
+  } else if constexpr (sizeof(S) == 4) {
+    if (c.rows == 20) {
+      switch (c.blt) {
+        case 1: return occupancy_of<S, 1, 20>();
+        case 2: return occupancy_of<S, 2, 20>();
+        case 3: return occupancy_of<S, 3, 20>();
+      }
+    } else if (c.rows == 24) {
+      switch (c.blt) {
+        case 1: return occupancy_of<S, 1, 24>();
+        case 2: return occupancy_of<S, 2, 24>();
+      }
+    }
   }
   return 1;
 }
@@ -591,11 +626,11 @@ int batch_occupancy_type(const TiledConfig& c) {
 
 bool tiled2_config_supported(const TiledConfig& c) {
   if (c.esz != 4 && c.esz != 2) return false;
-  if (c.rows != 8 && c.rows != 16 && c.rows != 32) return false;
-  if (c.rows == 32 && c.esz != 4) return false;
+  if (c.rows != 8 && c.rows != 16 && c.rows != 20 && c.rows != 24 && c.rows != 32) return false;
+  if (c.rows > 16 && c.esz != 4) return false;
   if (c.blt < 1 || c.blt > 4) return false;
-  if (c.rows == 8 && c.blt > 3) return false;
-  if (c.rows == 32 && c.blt > 2) return false;  // 1024 threads: the pair state spills
+  if ((c.rows == 8 || c.rows == 20) && c.blt > 3) return false;
+  if ((c.rows == 24 || c.rows == 32) && c.blt > 2) return false;  // the pair state spills
   if (c.min_blocks > 1 && !(c.esz == 4 && c.blt == 2 &&
                             ((c.rows == 16 && c.min_blocks == 2) ||
                              (c.rows == 8 && c.min_blocks == 4))))
@@ -607,6 +642,8 @@ bool tiled2_batch_supported(const TiledConfig& c) {
   if (c.esz != 4 && c.esz != 2) return false;
   if (c.rows == 16) return c.blt >= 1 && c.blt <= 4;
   if (c.rows == 8) return c.blt >= 1 && c.blt <= 3;
+  if (c.rows == 20) return c.esz == 4 && c.blt >= 1 && c.blt <= 3;
+  if (c.rows == 24) return c.esz == 4 && c.blt >= 1 && c.blt <= 2;
   return false;
 }
 
@@ -634,6 +671,17 @@ size_t tiled2_batch_smem(const TiledConfig& c) {
       case 1: return h ? smem_of<__half, 1, 8>() : smem_of<float, 1, 8>();
       case 2: return h ? smem_of<__half, 2, 8>() : smem_of<float, 2, 8>();
       case 3: return h ? smem_of<__half, 3, 8>() : smem_of<float, 3, 8>();
+    }
+  } else if (c.rows == 20 && !h) {
+    switch (c.blt) {
+      case 1: return smem_of<float, 1, 20>();
+      case 2: return smem_of<float, 2, 20>();
+      case 3: return smem_of<float, 3, 20>();
+    }
+  } else if (c.rows == 24 && !h) {
+    switch (c.blt) {
+      case 1: return smem_of<float, 1, 24>();
+      case 2: return smem_of<float, 2, 24>();
     }
   }
   return 0;

@@ -86,7 +86,8 @@ typedef struct fdtd_desc {
   int32_t storage;      /* fdtd_storage */
   int32_t kernel;       /* fdtd_kernel */
   int32_t blt;          /* time steps per tiled launch; 0 = autotuned */
-  int32_t tile_rows;    /* tiled-kernel rows per tile (8, 16 or 32); 0 = autotuned */
+  int32_t tile_rows;    /* tiled-kernel rows per tile (8, 16, 20, 24 or 32; 20 and 24 for the
+                           FP32 x-pair kernel only); 0 = autotuned */
   int32_t z_chunks;     /* tiled-kernel z-chunks per column; 0 = autotuned */
   int32_t min_blocks;   /* tiled x-pair family: CTAs per SM the registers must allow (1, 2 or
                            4); 0 = autotuned */
