@@ -111,23 +111,23 @@ class ClockSampler:
 
 
 def traffic_from_profile(cfg):
-    """DRAM bytes per launch of the tiled kernel from the committed ncu summary, if the
-    summary's configuration matches the one running now."""
+    """DRAM bytes per launch of the tiled kernel from the committed ncu summary (one line per
+    configuration), if one of its configurations is the one running now."""
     p = os.path.join(ROOT, "profiles", "fdtd_tiled_256cube_traffic.txt")
     if not os.path.exists(p):
         return None
-    kv = {}
     for ln in open(p):
-        if "=" in ln and not ln.startswith("#"):
-            k, v = ln.split("=", 1)
-            kv[k.strip()] = v.strip()
-    try:
-        if (int(kv["blt"]), int(kv["tile_rows"]), int(kv["z_chunks"])) != \
-                (cfg["blt"], cfg["tile_rows"], cfg["z_chunks"]):
-            return None
-        return float(kv["dram_bytes_per_launch"])
-    except (KeyError, ValueError):
-        return None
+        ln = ln.split("#", 1)[0].strip()
+        if not ln:
+            continue
+        kv = dict(part.split("=", 1) for part in ln.split() if "=" in part)
+        try:
+            if (int(kv["blt"]), int(kv["tile_rows"]), int(kv["z_chunks"])) == \
+                    (cfg["blt"], cfg["tile_rows"], cfg["z_chunks"]):
+                return float(kv["dram_bytes_per_launch"])
+        except (KeyError, ValueError):
+            continue
+    return None
 
 
 # ------------------------------------------------------------------ reference arm / CPU
