@@ -11,8 +11,9 @@
 //
 // Two GEMM paths compute the same products: tcgen05.mma with a TMEM accumulator (mlp_tc.cu) and
 // the warp-level mma.sync.m16n8k16 kernel below.  The default (AUTO) runs products of >= 1024
-// rows (inference) on the first and the 64-row minibatch products of training on the second;
-// fdtd_mlp_set_gemm forces either (the tests cross-check them).
+// rows on the first and the 64-row minibatch products of training on the second;
+// fdtd_mlp_set_gemm forces either (the tests cross-check them).  Inference (predict) on the
+// tcgen05 path runs all layers in one fused kernel when the widths allow (mlp_tc.cu).
 //
 // GEMM: C[M][N] = sum_k opA(m,k) opB(n,k), opX(r,k) = TX ? X[k*ld + r] : X[r*ld + k], so one
 // kernel serves the forward pass (X W^T), the input gradient (G W) and the weight gradient
@@ -486,11 +487,33 @@ fdtd_status predict_rows(fdtd_mlp* m, const float* x_dev, long long n, float* me
   const long long chunk = std::min<long long>(n, 65536);
   fdtd_status s = ensure_cap(m, chunk);
   if (s != FDTD_OK) return s;
+  const bool fused = m->gemm_kind != FDTD_MLP_GEMM_MMA_SYNC && m->L <= fdtd::mlp::kFusedMaxLayers &&
+                     fdtd::mlp::mlp_fused_supported(m->dims.data(), m->L);
   for (long long r0 = 0; r0 < n; r0 += chunk) {
     const long long cnt = std::min<long long>(chunk, n - r0);
-    fdtd::mlp::to_bf16<<<fdtd::mlp::nblocks(cnt * in), 256, 0, m->st>>>(cnt * in, x_dev + r0 * in,
-                                                                         m->act[0]);
-    forward(m, (int)cnt, 0, /*keep_z=*/false);
+    if (fused) {  // every layer in one kernel: activations never leave the SM
+      fdtd::mlp::FusedArgs fa{};
+      fa.x = x_dev + r0 * in;
+      fa.n = cnt;
+      fa.L = m->L;
+      for (int l = 0; l <= m->L; ++l) fa.dims[l] = m->dims[l];
+      for (int l = 0; l < m->L; ++l) {
+        fa.w_off[l] = m->w_off[l];
+        fa.b_off[l] = m->b_off[l];
+      }
+      fa.wbf = m->wbf;
+      fa.params = m->params;
+      fa.P = m->P;
+      fa.out = m->z[m->L - 1];
+      fa.out_stride = m->cap * out;
+      fa.err = m->d_err;
+      const cudaError_t le = fdtd::mlp::launch_mlp_fused(fa, m->E, m->st);
+      if (le != cudaSuccess && m->launch_err == cudaSuccess) m->launch_err = le;
+    } else {
+      fdtd::mlp::to_bf16<<<fdtd::mlp::nblocks(cnt * in), 256, 0, m->st>>>(
+          cnt * in, x_dev + r0 * in, m->act[0]);
+      forward(m, (int)cnt, 0, /*keep_z=*/false);
+    }
     fdtd::mlp::ens_stats<<<fdtd::mlp::nblocks(cnt * out), 256, 0, m->st>>>(
         cnt * out, m->E, m->z[m->L - 1], m->cap * out, mean + r0 * out, sd + r0 * out);
     if (per_member)

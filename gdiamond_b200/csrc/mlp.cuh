@@ -49,6 +49,25 @@ __device__ __forceinline__ void epilogue_store(const Epilogue& ep, int e, int r,
   if (EPI == kGeluBack) ep.out_bf[e * ep.stride_out + o] = __float2bfloat16_rn(v);
 }
 
+// Fused ensemble inference (mlp_tc.cu): every layer of one member for 128 rows per CTA.
+constexpr int kFusedMaxLayers = 8;
+struct FusedArgs {
+  const float* x;                  // [n][dims[0]] FP32 inputs
+  long long n;
+  int L;                           // layers
+  int dims[kFusedMaxLayers + 1];
+  long long w_off[kFusedMaxLayers], b_off[kFusedMaxLayers];
+  const __nv_bfloat16* wbf;        // [members][P] BF16 weights
+  const float* params;             // [members][P] FP32 parameters (biases)
+  long long P;
+  float* out;                      // [members][out_stride]: [n][dims[L]] per member
+  long long out_stride;
+  int* err;
+};
+// dims[0] <= 64; every other width a multiple of 64 up to 256.
+bool mlp_fused_supported(const int* dims, int L);
+cudaError_t launch_mlp_fused(const FusedArgs& a, int members, cudaStream_t st);
+
 // tcgen05 GEMM (mlp_tc.cu): C[M][N] (+epilogue) for `members` members on `st`; `err` receives
 // a nonzero word if a bounded wait inside the kernel gave up.  Instantiated for the epilogues
 // the MLP uses (mlp_tc.cu lists them).

@@ -302,6 +302,195 @@ cudaError_t launch_bn(int M, int N, int K, const Operand& A, const Operand& B, c
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------- fused ensemble inference
+// One CTA of 256 threads takes 128 rows of one member through every layer: the BF16 activations
+// stay in shared memory as the next layer's A operand (a 128 x 256 K-major core-matrix tile,
+// 8-row groups 4096 B apart), the weights stream through two 64-wide K stages (N x 64 core
+// matrices), the FP32 accumulator (up to 256 columns) stays in TMEM, and only the last layer's
+// output is written to global memory.
+
+constexpr int FACT_K = 256;  // widest layer input held in the activation tile
+constexpr int FROWS = 128;
+constexpr int FTHREADS = 256;
+constexpr uint32_t F_ACT_BYTES = FROWS * FACT_K * 2;   // 64 KB
+constexpr uint32_t F_W_BYTES = 256 * TBK * 2;          // 32 KB per weight stage
+constexpr uint32_t F_SMEM = F_ACT_BYTES + 2 * F_W_BYTES + 64 + 1024;
+
+__device__ __forceinline__ uint32_t act_off(int r, int k) {
+  return (uint32_t)(((((r >> 3) * (FACT_K / 8)) + (k >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+__device__ __forceinline__ uint64_t smem_desc_sbo(uint32_t saddr, uint32_t sbo_bytes) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(sbo_bytes >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ uint32_t instr_desc_n(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(FROWS >> 4) << 24);  // M = 128 rows
+}
+
+// One thread's share of an N x 64 weight chunk (N <= 256): up to 8 chunks of 8 BF16.
+struct WChunk {
+  uint4 v[8];
+};
+
+__device__ __forceinline__ void load_w(WChunk& c, const __nv_bfloat16* W, int N, int K, int k0) {
+  const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+  const bool vec = (K % 8) == 0;
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int id = threadIdx.x + it * FTHREADS;
+    const int n = (id >> 6) * 8 + (id & 7), k = ((id >> 3) & 7) * 8;
+    if (n >= N) continue;
+    const int gk = k0 + k;
+    if (vec && gk + 8 <= K) {
+      c.v[it] = *reinterpret_cast<const uint4*>(W + (long long)n * K + gk);
+    } else {
+      __nv_bfloat16 e[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) e[q] = gk + q < K ? W[(long long)n * K + gk + q] : zero;
+      memcpy(&c.v[it], e, 16);
+    }
+  }
+}
+
+__device__ __forceinline__ void store_w(uint8_t* s, const WChunk& c, int N) {
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int id = threadIdx.x + it * FTHREADS;
+    const int n = (id >> 6) * 8 + (id & 7), k = ((id >> 3) & 7) * 8;
+    if (n < N) *reinterpret_cast<uint4*>(s + cm_off(n, k)) = c.v[it];
+  }
+}
+
+__global__ void __launch_bounds__(FTHREADS, 1) mlp_fused_infer(FusedArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                           ~static_cast<uintptr_t>(1023));
+  uint8_t* act = sm;
+  uint8_t* sW = sm + F_ACT_BYTES;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sW + 2 * F_W_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int e = blockIdx.y;
+  const long long m0 = (long long)blockIdx.x * FROWS;
+  const __nv_bfloat16* wbf = a.wbf + e * a.P;
+  const float* prm = a.params + e * a.P;
+
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, 256);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  // inputs (FP32 [n][in], in <= 64) -> BF16 columns 0..63 of the activation tile
+  for (int q = tid; q < FROWS * 64; q += FTHREADS) {
+    const int r = q >> 6, k = q & 63;
+    const long long row = m0 + r;
+    float v = 0.0f;
+    if (row < a.n && k < a.dims[0]) v = a.x[row * a.dims[0] + k];
+    *reinterpret_cast<__nv_bfloat16*>(act + act_off(r, k)) = __float2bfloat16_rn(v);
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  WChunk pre;
+  load_w(pre, wbf + a.w_off[0], a.dims[1], a.dims[0], 0);
+  int g = 0;  // weight chunks committed so far; stage = g & 1
+  bool failed = false;
+  for (int l = 0; l < a.L && !failed; ++l) {
+    const int K = a.dims[l], N = a.dims[l + 1];
+    const int nch = (K + TBK - 1) / TBK;
+    for (int c = 0; c < nch; ++c) {
+      const int s = g & 1;
+      bool bad = false;
+      if (g >= 2 && !mbar_wait_bounded(&bar[s], ((g - 2) >> 1) & 1, kTcWaitLimit)) {
+        bad = true;
+        atomicExch(a.err, 1);
+      }
+      if (!bad) store_w(sW + s * F_W_BYTES, pre, N);
+      fence_proxy_async_smem();
+      if (__syncthreads_or(bad)) {
+        failed = true;
+        break;
+      }
+      if (c + 1 < nch)
+        load_w(pre, wbf + a.w_off[l], N, K, (c + 1) * TBK);
+      else if (l + 1 < a.L)
+        load_w(pre, wbf + a.w_off[l + 1], a.dims[l + 2], a.dims[l + 1], 0);
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t a0 = smem_u32(act), b0 = smem_u32(sW + s * F_W_BYTES);
+#pragma unroll
+        for (int j = 0; j < TBK / 16; ++j)
+          umma_bf16(tmem, smem_desc_sbo(a0 + (uint32_t)(c * 8 + 2 * j) * 128u, FACT_K / 8 * 128),
+                    smem_desc_sbo(b0 + (uint32_t)j * 256u, TBK / 8 * 128), instr_desc_n(N),
+                    (c > 0 || j > 0) ? 1u : 0u);
+        umma_commit(&bar[s]);
+      }
+      ++g;
+    }
+    if (failed) break;
+    bool late = !mbar_wait_bounded(&bar[(g - 1) & 1], ((g - 1) >> 1) & 1, kTcWaitLimit);
+    if (late) atomicExch(a.err, 1);
+    if (__syncthreads_or(late)) {
+      failed = true;
+      break;
+    }
+    tc_fence_after();
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (tile rows), column half w / 4
+    const int q4 = warp & 3, half = warp >> 2;
+    const int r = q4 * 32 + lane;
+    const long long row = m0 + r;
+    const float* bias = prm + a.b_off[l];
+    const bool last = l + 1 == a.L;
+#pragma unroll 1
+    for (int c0 = half * (N / 2); c0 < (half + 1) * (N / 2); c0 += 32) {
+      uint32_t v[32];
+      tmem_ld32(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)c0, v);
+      tmem_wait_ld();
+      if (!last) {
+#pragma unroll
+        for (int q = 0; q < 32; q += 8) {
+          __nv_bfloat16 h[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            h[u] = __float2bfloat16_rn(gelu(__uint_as_float(v[q + u]) + bias[c0 + q + u]));
+          uint4 w;
+          memcpy(&w, h, 16);
+          *reinterpret_cast<uint4*>(act + act_off(r, c0 + q)) = w;
+        }
+      } else if (row < a.n) {
+        float* o = a.out + e * a.out_stride + row * N + c0;
+#pragma unroll
+        for (int q = 0; q < 32; q += 4)
+          *reinterpret_cast<float4*>(o + q) =
+              make_float4(__uint_as_float(v[q]) + bias[c0 + q], __uint_as_float(v[q + 1]) + bias[c0 + q + 1],
+                          __uint_as_float(v[q + 2]) + bias[c0 + q + 2],
+                          __uint_as_float(v[q + 3]) + bias[c0 + q + 3]);
+      }
+    }
+    fence_proxy_async_smem();  // the new activations are the next MMAs' operand
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
+  if (failed && g > 0) {  // let what was issued finish before the accumulator is released
+    (void)mbar_wait_bounded(&bar[(g - 1) & 1], ((g - 1) >> 1) & 1, kTcWaitLimit);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
 }  // namespace
 
 template <bool TA, bool TB, int EPI>
@@ -329,6 +518,30 @@ template cudaError_t launch_gemm_tc<true, true, kStore>(int, int, int, const Ope
 template cudaError_t launch_gemm_tc<false, true, kGeluBack>(int, int, int, const Operand&,
                                                             const Operand&, const Epilogue&, int,
                                                             cudaStream_t, int*);
+
+bool mlp_fused_supported(const int* dims, int L) {
+  if (L < 1 || L > kFusedMaxLayers || dims[0] < 1 || dims[0] > 64) return false;
+  for (int l = 1; l <= L; ++l)
+    if (dims[l] < 64 || dims[l] > FACT_K || dims[l] % 64 != 0) return false;
+  return true;
+}
+
+cudaError_t launch_mlp_fused(const FusedArgs& a, int members, cudaStream_t st) {
+  static unsigned long long set_on = 0;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+  if (!(set_on & bit) || !bit) {
+    e = cudaFuncSetAttribute(mlp_fused_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)F_SMEM);
+    if (e != cudaSuccess) return e;
+    set_on |= bit;
+  }
+  const dim3 grid((unsigned)((a.n + FROWS - 1) / FROWS), (unsigned)members);
+  mlp_fused_infer<<<grid, FTHREADS, F_SMEM, st>>>(a);
+  return cudaGetLastError();
+}
 
 }  // namespace mlp
 }  // namespace fdtd

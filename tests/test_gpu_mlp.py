@@ -164,3 +164,20 @@ def test_invalid_arguments():
     with pytest.raises(ValueError):
         net.set_data(np.zeros((3, 4)), np.zeros((2, 2)))
     net.close()
+
+
+@pytest.mark.parametrize("n", [1, 127, 129, 70000])
+def test_fused_inference_matches_layer_by_layer(n):
+    """predict() on the tcgen05 path runs every layer in one kernel (activations kept in shared
+    memory); the warp-level path runs the layers one GEMM at a time."""
+    dims = (6, 256, 256, 256, 64)
+    x, _ = data(n, dims, 11)
+    out = {}
+    for gemm in ("tcgen05", "mma_sync"):
+        net = gd.MLP(dims, members=4, seed=8, gemm=gemm)
+        out[gemm] = net.predict(x, members=True)
+        net.close()
+    (m1, s1, p1), (m0, s0, p0) = out["tcgen05"], out["mma_sync"]
+    assert np.all(np.isfinite(p1))
+    assert rel(p1, p0) <= 1e-3, rel(p1, p0)
+    assert rel(m1, m0) <= 1e-3
