@@ -49,7 +49,7 @@ __device__ __forceinline__ void epilogue_store(const Epilogue& ep, int e, int r,
   if (EPI == kGeluBack) ep.out_bf[e * ep.stride_out + o] = __float2bfloat16_rn(v);
 }
 
-// Fused ensemble inference (mlp_tc.cu): every layer of one member for 128 rows per CTA.
+// Fused ensemble inference (mlp_tc.cu): every layer of one member for 256 rows per CTA.
 constexpr int kFusedMaxLayers = 8;
 struct FusedArgs {
   const float* x;                  // [n][dims[0]] FP32 inputs
@@ -64,7 +64,7 @@ struct FusedArgs {
   long long out_stride;
   int* err;
 };
-// dims[0] <= 64; every other width a multiple of 64 up to 256.
+// dims[0] <= 64; every other width a multiple of 32 up to 256.
 bool mlp_fused_supported(const int* dims, int L);
 cudaError_t launch_mlp_fused(const FusedArgs& a, int members, cudaStream_t st);
 

@@ -303,18 +303,20 @@ cudaError_t launch_bn(int M, int N, int K, const Operand& A, const Operand& B, c
 }
 
 // ------------------------------------------------------------------- fused ensemble inference
-// One CTA of 256 threads takes 128 rows of one member through every layer: the BF16 activations
-// stay in shared memory as the next layer's A operand (a 128 x 256 K-major core-matrix tile,
-// 8-row groups 4096 B apart), the weights stream through two 64-wide K stages (N x 64 core
-// matrices), the FP32 accumulator (up to 256 columns) stays in TMEM, and only the last layer's
-// output is written to global memory.
+// One CTA of 256 threads takes 256 rows (two 128-row tiles) of one member through every layer:
+// the BF16 activations stay in shared memory as the next layer's A operand (one 128 x 256 K-major
+// core-matrix tile per row tile, 8-row groups 4096 B apart), the weights stream through two
+// 64-wide K stages (N x 64 core matrices) and each staged chunk feeds both row tiles, the FP32
+// accumulators (up to 2 x 256 columns) stay in TMEM, and only the last layer's output is written
+// to global memory.  Warps 0-3 run the epilogue of tile 0, warps 4-7 that of tile 1.
 
 constexpr int FACT_K = 256;  // widest layer input held in the activation tile
-constexpr int FROWS = 128;
+constexpr int FROWS = 128;                             // rows of one tile (the MMA's M)
+constexpr int FTILES = 2;                              // row tiles per CTA
 constexpr int FTHREADS = 256;
-constexpr uint32_t F_ACT_BYTES = FROWS * FACT_K * 2;   // 64 KB
+constexpr uint32_t F_ACT_BYTES = FROWS * FACT_K * 2;   // 64 KB per row tile
 constexpr uint32_t F_W_BYTES = 256 * TBK * 2;          // 32 KB per weight stage
-constexpr uint32_t F_SMEM = F_ACT_BYTES + 2 * F_W_BYTES + 64 + 1024;
+constexpr uint32_t F_SMEM = FTILES * F_ACT_BYTES + 2 * F_W_BYTES + 64 + 1024;
 
 __device__ __forceinline__ uint32_t act_off(int r, int k) {
   return (uint32_t)(((((r >> 3) * (FACT_K / 8)) + (k >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
@@ -368,19 +370,19 @@ __global__ void __launch_bounds__(FTHREADS, 1) mlp_fused_infer(FusedArgs a) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                            ~static_cast<uintptr_t>(1023));
-  uint8_t* act = sm;
-  uint8_t* sW = sm + F_ACT_BYTES;
+  uint8_t* act = sm;  // [FTILES][F_ACT_BYTES]
+  uint8_t* sW = sm + FTILES * F_ACT_BYTES;
   uint64_t* bar = reinterpret_cast<uint64_t*>(sW + 2 * F_W_BYTES);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int e = blockIdx.y;
-  const long long m0 = (long long)blockIdx.x * FROWS;
+  const long long m0 = (long long)blockIdx.x * (FROWS * FTILES);
   const __nv_bfloat16* wbf = a.wbf + e * a.P;
   const float* prm = a.params + e * a.P;
 
   if (warp == 0) {
-    tmem_alloc(tmem_slot, 256);
+    tmem_alloc(tmem_slot, 256 * FTILES);
     tmem_relinquish();
   }
   if (tid == 0) {
@@ -389,12 +391,13 @@ __global__ void __launch_bounds__(FTHREADS, 1) mlp_fused_infer(FusedArgs a) {
     fence_mbar_init();
   }
   // inputs (FP32 [n][in], in <= 64) -> BF16 columns 0..63 of the activation tile
-  for (int q = tid; q < FROWS * 64; q += FTHREADS) {
-    const int r = q >> 6, k = q & 63;
+  for (int q = tid; q < FTILES * FROWS * 64; q += FTHREADS) {
+    const int r = q >> 6, k = q & 63;  // r: row of the CTA, tile r / FROWS
     const long long row = m0 + r;
     float v = 0.0f;
     if (row < a.n && k < a.dims[0]) v = a.x[row * a.dims[0] + k];
-    *reinterpret_cast<__nv_bfloat16*>(act + act_off(r, k)) = __float2bfloat16_rn(v);
+    *reinterpret_cast<__nv_bfloat16*>(act + (r / FROWS) * F_ACT_BYTES + act_off(r % FROWS, k)) =
+        __float2bfloat16_rn(v);
   }
   fence_proxy_async_smem();
   tc_fence_before();
@@ -428,12 +431,17 @@ __global__ void __launch_bounds__(FTHREADS, 1) mlp_fused_infer(FusedArgs a) {
         load_w(pre, wbf + a.w_off[l + 1], a.dims[l + 2], a.dims[l + 1], 0);
       if (tid == 0) {
         tc_fence_after();
-        const uint32_t a0 = smem_u32(act), b0 = smem_u32(sW + s * F_W_BYTES);
+        const uint32_t b0 = smem_u32(sW + s * F_W_BYTES);
 #pragma unroll
-        for (int j = 0; j < TBK / 16; ++j)
-          umma_bf16(tmem, smem_desc_sbo(a0 + (uint32_t)(c * 8 + 2 * j) * 128u, FACT_K / 8 * 128),
-                    smem_desc_sbo(b0 + (uint32_t)j * 256u, TBK / 8 * 128), instr_desc_n(N),
-                    (c > 0 || j > 0) ? 1u : 0u);
+        for (int t = 0; t < FTILES; ++t) {
+          const uint32_t a0 = smem_u32(act + t * F_ACT_BYTES);
+#pragma unroll
+          for (int j = 0; j < TBK / 16; ++j)
+            umma_bf16(tmem + (uint32_t)(t * 256), smem_desc_sbo(a0 + (uint32_t)(c * 8 + 2 * j) * 128u,
+                                                                 FACT_K / 8 * 128),
+                      smem_desc_sbo(b0 + (uint32_t)j * 256u, TBK / 8 * 128), instr_desc_n(N),
+                      (c > 0 || j > 0) ? 1u : 0u);
+        }
         umma_commit(&bar[s]);
       }
       ++g;
@@ -446,16 +454,17 @@ __global__ void __launch_bounds__(FTHREADS, 1) mlp_fused_infer(FusedArgs a) {
       break;
     }
     tc_fence_after();
-    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (tile rows), column half w / 4
-    const int q4 = warp & 3, half = warp >> 2;
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows of its tile) of tile w / 4
+    const int q4 = warp & 3, t = warp >> 2;
     const int r = q4 * 32 + lane;
-    const long long row = m0 + r;
+    const long long row = m0 + t * FROWS + r;
+    uint8_t* tact = act + t * F_ACT_BYTES;
     const float* bias = prm + a.b_off[l];
     const bool last = l + 1 == a.L;
 #pragma unroll 1
-    for (int c0 = half * (N / 2); c0 < (half + 1) * (N / 2); c0 += 32) {
+    for (int c0 = 0; c0 < N; c0 += 32) {
       uint32_t v[32];
-      tmem_ld32(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)c0, v);
+      tmem_ld32(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(t * 256 + c0), v);
       tmem_wait_ld();
       if (!last) {
 #pragma unroll
@@ -466,7 +475,7 @@ __global__ void __launch_bounds__(FTHREADS, 1) mlp_fused_infer(FusedArgs a) {
             h[u] = __float2bfloat16_rn(gelu(__uint_as_float(v[q + u]) + bias[c0 + q + u]));
           uint4 w;
           memcpy(&w, h, 16);
-          *reinterpret_cast<uint4*>(act + act_off(r, c0 + q)) = w;
+          *reinterpret_cast<uint4*>(tact + act_off(r, c0 + q)) = w;
         }
       } else if (row < a.n) {
         float* o = a.out + e * a.out_stride + row * N + c0;
@@ -488,7 +497,7 @@ __global__ void __launch_bounds__(FTHREADS, 1) mlp_fused_infer(FusedArgs a) {
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 256);
+  if (warp == 0) tmem_dealloc(tmem, 256 * FTILES);
 }
 
 }  // namespace
@@ -522,7 +531,7 @@ template cudaError_t launch_gemm_tc<false, true, kGeluBack>(int, int, int, const
 bool mlp_fused_supported(const int* dims, int L) {
   if (L < 1 || L > kFusedMaxLayers || dims[0] < 1 || dims[0] > 64) return false;
   for (int l = 1; l <= L; ++l)
-    if (dims[l] < 64 || dims[l] > FACT_K || dims[l] % 64 != 0) return false;
+    if (dims[l] < 32 || dims[l] > FACT_K || dims[l] % 32 != 0) return false;
   return true;
 }
 
@@ -538,7 +547,7 @@ cudaError_t launch_mlp_fused(const FusedArgs& a, int members, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     set_on |= bit;
   }
-  const dim3 grid((unsigned)((a.n + FROWS - 1) / FROWS), (unsigned)members);
+  const dim3 grid((unsigned)((a.n + FROWS * FTILES - 1) / (FROWS * FTILES)), (unsigned)members);
   mlp_fused_infer<<<grid, FTHREADS, F_SMEM, st>>>(a);
   return cudaGetLastError();
 }
