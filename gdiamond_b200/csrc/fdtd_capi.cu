@@ -1005,6 +1005,10 @@ struct fdtd_batch {
   bool cfg_ready = false;
   fdtd::TiledArgs* d_args = nullptr;  // [2][n]
   fdtd::TiledArgs* h_args = nullptr;  // pinned staging [2][n]
+  // Recorded after each step's launches: the copy of h_args (a graph node or an asynchronous
+  // copy) has run once it completes, so the next step may refill h_args.
+  cudaEvent_t args_read = nullptr;
+  bool args_pending = false;
   std::map<int, std::pair<int4*, int>> items;  // per BLT: device work items, count
   unsigned int* d_counters = nullptr;
   int counters_cap = 0;
@@ -1253,6 +1257,7 @@ fdtd_status fdtd_batch_destroy(fdtd_batch* b) {
   cudaFree(b->d_counters);
   cudaFree(b->d_args);
   if (b->h_args) cudaFreeHost(b->h_args);
+  if (b->args_read) cudaEventDestroy(b->args_read);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return FDTD_OK;
@@ -1264,6 +1269,10 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
   DeviceGuard dg(b->device);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
   fdtd_status s;
+  if (b->args_pending) {  // the previous step's copy of h_args must have run before a refill
+    BCUDA(b, cudaEventSynchronize(b->args_read));
+    b->args_pending = false;
+  }
   for (fdtd_handle* h : b->sims) {
     if ((s = ensure_tables(h, h->t + T)) != FDTD_OK) return bfail(b, s, "%s", h->err.c_str());
     if ((s = stream_after(b, st, h->stream)) != FDTD_OK) return s;
@@ -1324,6 +1333,9 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
   } else {
     if ((s = record(st)) != FDTD_OK) return s;
   }
+  if (!b->args_read) BCUDA(b, cudaEventCreateWithFlags(&b->args_read, cudaEventDisableTiming));
+  BCUDA(b, cudaEventRecord(b->args_read, st));
+  b->args_pending = true;
   for (fdtd_handle* h : b->sims) {
     h->t += T;
     h->cur ^= (nl & 1);

@@ -215,3 +215,22 @@ def test_batch_rejects_mixed_storage():
         gd.Batch([a, c])
     for s in (a, b, c):
         s.close()
+
+
+def test_batch_back_to_back_steps_without_sync():
+    """Two batch steps issued without a synchronisation between them (graph and plain): the
+    second must not change the arguments the first one is still to read."""
+    T = 6
+    for use_graph in (True, False):
+        sims, refs = make_batch("f32", 2 * T)
+        batch = gd.Batch(sims)
+        batch.step(T, use_graph=use_graph)
+        batch.step(T, use_graph=use_graph)
+        for sim, (shape, coefs, src, mons) in zip(sims, refs):
+            F_ref = oracle.run(shape, coefs, 2 * T, sources=[osrc(s) for s in src])
+            sim.sync()
+            for c, f in enumerate(sim.fields()):
+                assert bits_equal(f, F_ref[c]), (use_graph, shape, oracle.COMPONENTS[c])
+        batch.close()
+        for sim in sims:
+            sim.close()
