@@ -18,6 +18,8 @@
 // Every mbarrier wait is bounded; on expiry the kernel records an error word, stops issuing
 // (decided block-wide with __syncthreads_or), waits (bounded) for what it issued, skips the
 // epilogue, frees its TMEM and returns.
+#include <atomic>
+
 #include "fdtd_common.cuh"
 #include "mlp.cuh"
 
@@ -286,16 +288,16 @@ __global__ void __launch_bounds__(128) gemm_tc(int M, int N, int K, Operand A, O
 template <bool TA, bool TB, int EPI, int BN>
 cudaError_t launch_bn(int M, int N, int K, const Operand& A, const Operand& B, const Epilogue& ep,
                       int members, cudaStream_t st, int* err) {
-  static unsigned long long set_on = 0;  // devices (bit per ordinal < 64) with the attribute set
+  static std::atomic<unsigned long long> set_on{0};  // devices (bit per ordinal < 64) done
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
-  if (!(set_on & bit) || !bit) {
+  if (!(set_on.load() & bit) || !bit) {
     e = cudaFuncSetAttribute(gemm_tc<TA, TB, EPI, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TcSmem<BN>::BYTES);
     if (e != cudaSuccess) return e;
-    set_on |= bit;
+    set_on.fetch_or(bit);
   }
   const dim3 grid((N + BN - 1) / BN, (M + TBM - 1) / TBM, members);
   gemm_tc<TA, TB, EPI, BN><<<grid, 128, TcSmem<BN>::BYTES, st>>>(M, N, K, A, B, ep, err);
@@ -536,16 +538,16 @@ bool mlp_fused_supported(const int* dims, int L) {
 }
 
 cudaError_t launch_mlp_fused(const FusedArgs& a, int members, cudaStream_t st) {
-  static unsigned long long set_on = 0;
+  static std::atomic<unsigned long long> set_on{0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
-  if (!(set_on & bit) || !bit) {
+  if (!(set_on.load() & bit) || !bit) {
     e = cudaFuncSetAttribute(mlp_fused_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)F_SMEM);
     if (e != cudaSuccess) return e;
-    set_on |= bit;
+    set_on.fetch_or(bit);
   }
   const dim3 grid((unsigned)((a.n + FROWS * FTILES - 1) / (FROWS * FTILES)), (unsigned)members);
   mlp_fused_infer<<<grid, FTHREADS, F_SMEM, st>>>(a);
