@@ -725,7 +725,7 @@ def main():
     ap.add_argument("--grid", default="256,256,256", help="NX,NY,NZ (profiling cases)")
     ap.add_argument("--timesteps", type=int, default=T_STEPS)
     ap.add_argument("--kernel", default="auto",
-                    choices=["auto", "naive", "tiled", "tiled_w32", "tiled_w64"])
+                    choices=["auto", "naive", "tiled", "tiled_w32", "tiled_w64", "tiled_w32p"])
     ap.add_argument("--blt", type=int, default=0, help="force time steps per launch")
     ap.add_argument("--rows", type=int, default=0, help="force tile rows")
     ap.add_argument("--zchunks", type=int, default=0, help="force z-chunks")

@@ -22,7 +22,7 @@ LIB_PATH = os.path.join(_HERE, "libgdiamond_b200.so")
 COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 SOURCE_COMPONENTS = ("Jx", "Jy", "Jz", "Mx", "My", "Mz")
 COEFFS = ("Cax", "Cay", "Caz", "Cbx", "Cby", "Cbz", "Dax", "Day", "Daz", "Dbx", "Dby", "Dbz")
-KERNELS = {"auto": 0, "naive": 1, "tiled": 2, "tiled_w32": 3, "tiled_w64": 4}
+KERNELS = {"auto": 0, "naive": 1, "tiled": 2, "tiled_w32": 3, "tiled_w64": 4, "tiled_w32p": 5}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
 SRC_POINT, SRC_PLANE_Z = 0, 1
 
@@ -286,10 +286,11 @@ class Simulation:
     def config(self):
         out = (C.c_int32 * 6)()
         self._check(self._L.fdtd_get_config(self._h, out))
-        kernel = {1: "naive", 3: "tiled", 4: "tiled"}.get(out[0], "none")
-        width = {3: 32, 4: 64}.get(out[0], 0)
-        return {"kernel": kernel, "width": width, "blt": out[1], "tile_rows": out[2],
-                "z_chunks": out[3], "launches": out[4], "min_blocks": out[5]}
+        kernel = {1: "naive", 3: "tiled", 4: "tiled", 5: "tiled"}.get(out[0], "none")
+        width = {3: 32, 4: 64, 5: 32}.get(out[0], 0)
+        return {"kernel": kernel, "width": width, "pairs": out[0] in (4, 5), "blt": out[1],
+                "tile_rows": out[2], "z_chunks": out[3], "launches": out[4],
+                "min_blocks": out[5]}
 
     # ---------------------------------------------------------------- results
     def get_field(self, component, out=None):

@@ -180,11 +180,13 @@ fdtd_status ensure_maps(fdtd_handle* h, int width, int rows) {
 
 cudaError_t launch_any(const fdtd::TiledConfig& c, const fdtd::TiledArgs& a, const Grid& g,
                        cudaStream_t st) {
-  return c.width == 64 ? fdtd::launch_tiled2(c, a, g, st) : fdtd::launch_tiled(c, a, g, st);
+  return (c.width == 64 || c.pairs32) ? fdtd::launch_tiled2(c, a, g, st)
+                                       : fdtd::launch_tiled(c, a, g, st);
 }
 
 bool config_supported(const fdtd::TiledConfig& c) {
-  return c.width == 64 ? fdtd::tiled2_config_supported(c) : fdtd::tiled_config_supported(c);
+  return (c.width == 64 || c.pairs32) ? fdtd::tiled2_config_supported(c)
+                                       : fdtd::tiled_config_supported(c);
 }
 
 fdtd::Sources make_sources(const fdtd_handle* h) {
@@ -266,26 +268,31 @@ fdtd::TiledArgs make_tiled_args(fdtd_handle* h, const fdtd::TiledConfig& c, long
 // Candidate tiled configurations for the autotuner.
 std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
   std::vector<fdtd::TiledConfig> out;
-  std::vector<int> blts = {1, 2, 3, 4, 5, 6}, rows_l = {8, 16, 20, 24, 32}, zc = {1, 2, 4, 8};
-  std::vector<int> widths = {32, 64};
+  std::vector<int> blts = {1, 2, 3, 4, 5, 6}, rows_l = {8, 16, 20, 24, 32, 48};
+  std::vector<int> zc = {1, 2, 4, 8};
+  // kernel families: 0 one cell per thread (32-wide rows), 1 x-pairs in 64-wide rows,
+  // 2 x-pairs in 32-wide rows (two per warp)
+  std::vector<int> fams = {0, 1, 2};
   const bool half = h->esz == 2;
   if (half) {
-    widths = {64};
+    fams = {1};
     rows_l = {8, 16};
   }
   if (h->desc.blt > 0) blts = {h->desc.blt};
   if (h->desc.tile_rows > 0) rows_l = {h->desc.tile_rows};
   if (h->desc.z_chunks > 0) zc = {h->desc.z_chunks};
-  if (h->desc.kernel == FDTD_KERNEL_TILED_W32) widths = {32};
-  if (h->desc.kernel == FDTD_KERNEL_TILED_W64) widths = {64};
+  if (h->desc.kernel == FDTD_KERNEL_TILED_W32) fams = {0};
+  if (h->desc.kernel == FDTD_KERNEL_TILED_W64) fams = {1};
+  if (h->desc.kernel == FDTD_KERNEL_TILED_W32P) fams = {2};
   const bool forced_z = h->desc.z_chunks > 0;
-  for (int w : widths)
+  for (int fam : fams)
     for (int rows : rows_l)
       for (int b : blts)
         for (int z : zc)
           for (int mb : {1, 2, 4}) {
             if (h->desc.min_blocks > 0 && mb != h->desc.min_blocks) continue;
-            fdtd::TiledConfig c{b, rows, z, w, mb, h->storage, h->esz};
+            fdtd::TiledConfig c{b, rows, z, fam == 1 ? 64 : 32, mb, h->storage, h->esz};
+            c.pairs32 = fam == 2;
             if (!config_supported(c)) continue;
             // A chunk shorter than its 2*BLT warm-up is only worth it when asked for.
             if (!forced_z && (h->g.nz + z - 1) / z < 2 * b) continue;
@@ -497,10 +504,11 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "grid axis too large");
   if (d->storage < FDTD_STORE_F32 || d->storage > FDTD_STORE_F64)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "unknown storage %d", d->storage);
-  if (d->kernel < FDTD_KERNEL_AUTO || d->kernel > FDTD_KERNEL_TILED_W64)
+  if (d->kernel < FDTD_KERNEL_AUTO || d->kernel > FDTD_KERNEL_TILED_W32P)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "unknown kernel %d", d->kernel);
   if ((d->storage == FDTD_STORE_F16 || d->storage == FDTD_STORE_BF16) &&
-      (d->kernel == FDTD_KERNEL_NAIVE || d->kernel == FDTD_KERNEL_TILED_W32))
+      (d->kernel == FDTD_KERNEL_NAIVE || d->kernel == FDTD_KERNEL_TILED_W32 ||
+       d->kernel == FDTD_KERNEL_TILED_W32P))
     return fail(nullptr, FDTD_ERR_UNSUPPORTED,
                 "16-bit field storage runs the tiled x-pair kernel only");
   if (d->storage == FDTD_STORE_F64 && d->kernel != FDTD_KERNEL_AUTO &&
@@ -508,8 +516,8 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
     return fail(nullptr, FDTD_ERR_UNSUPPORTED, "FP64 field storage runs the naive kernel only");
   if (d->blt < 0 || d->blt > 6) return fail(nullptr, FDTD_ERR_INVALID_ARG, "blt must be 0..6");
   if (d->tile_rows != 0 && d->tile_rows != 8 && d->tile_rows != 16 && d->tile_rows != 20 &&
-      d->tile_rows != 24 && d->tile_rows != 32)
-    return fail(nullptr, FDTD_ERR_INVALID_ARG, "tile_rows must be 0, 8, 16, 20, 24 or 32");
+      d->tile_rows != 24 && d->tile_rows != 32 && d->tile_rows != 48)
+    return fail(nullptr, FDTD_ERR_INVALID_ARG, "tile_rows must be 0, 8, 16, 20, 24, 32 or 48");
   if (d->z_chunks < 0) return fail(nullptr, FDTD_ERR_INVALID_ARG, "z_chunks must be >= 0");
   if (d->min_blocks != 0 && d->min_blocks != 1 && d->min_blocks != 2 && d->min_blocks != 4)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "min_blocks must be 0, 1, 2 or 4");
@@ -783,7 +791,8 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
       h->t += cc.blt;
       left -= cc.blt;
     }
-    h->last_kernel = c.width == 64 ? FDTD_KERNEL_TILED_W64 : FDTD_KERNEL_TILED_W32;
+    h->last_kernel = c.pairs32 ? FDTD_KERNEL_TILED_W32P
+                               : (c.width == 64 ? FDTD_KERNEL_TILED_W64 : FDTD_KERNEL_TILED_W32);
   }
   h->last_launches = launches;
   if (st != h->stream) {
@@ -1040,8 +1049,9 @@ fdtd_status bfail(fdtd_batch* b, fdtd_status s, const char* fmt, ...) {
                    __LINE__);                                                             \
   } while (0)
 
-fdtd::TiledConfig batch_cfg(const fdtd_batch* b, int blt, int rows) {
-  fdtd::TiledConfig c{blt, rows, 1, 64, 1, b->storage, b->esz};
+fdtd::TiledConfig batch_cfg(const fdtd_batch* b, int blt, int rows, bool pairs32 = false) {
+  fdtd::TiledConfig c{blt, rows, 1, pairs32 ? 32 : 64, 1, b->storage, b->esz};
+  c.pairs32 = pairs32;
   return c;
 }
 
@@ -1051,7 +1061,7 @@ int sim_chunks(const Grid& g, int zlen) { return zlen <= 0 ? 1 : std::max(1, (g.
 // Work items of one (BLT, rows, chunk length): every z-chunk of every tile column of every
 // simulation, longest z-march first so the queue's tail is short.
 fdtd_status batch_items(fdtd_batch* b, const fdtd::TiledConfig& c, std::pair<int4*, int>* out) {
-  const int key = (b->zlen * 10 + c.blt) * 100 + c.rows;
+  const int key = ((b->zlen * 10 + c.blt) * 100 + c.rows) * 2 + (c.pairs32 ? 1 : 0);
   auto it = b->items.find(key);
   if (it != b->items.end()) {
     *out = it->second;
@@ -1083,9 +1093,9 @@ fdtd_status batch_items(fdtd_batch* b, const fdtd::TiledConfig& c, std::pair<int
   return FDTD_OK;
 }
 
-fdtd_status batch_maps(fdtd_batch* b, int rows) {
+fdtd_status batch_maps(fdtd_batch* b, const fdtd::TiledConfig& c) {
   for (fdtd_handle* h : b->sims) {
-    fdtd_status s = ensure_maps(h, 64, rows);
+    fdtd_status s = ensure_maps(h, c.width, c.rows);
     if (s != FDTD_OK) return bfail(b, s, "sim: %s", h->err.c_str());
   }
   return FDTD_OK;
@@ -1146,12 +1156,13 @@ fdtd_status batch_autotune(fdtd_batch* b, cudaStream_t st) {
     if (h->desc.tile_rows != want_rows) want_rows = 0;
   }
   std::vector<fdtd::TiledConfig> cands;
-  for (int rows : {16, 8, 20, 24})
-    for (int blt = 1; blt <= 4; ++blt) {
-      if ((want_blt > 0 && blt != want_blt) || (want_rows > 0 && rows != want_rows)) continue;
-      fdtd::TiledConfig c = batch_cfg(b, blt, rows);
-      if (fdtd::tiled2_batch_supported(c)) cands.push_back(c);
-    }
+  for (int pairs32 = 0; pairs32 < 2; ++pairs32)
+    for (int rows : {16, 8, 20, 24, 32, 48})
+      for (int blt = 1; blt <= 4; ++blt) {
+        if ((want_blt > 0 && blt != want_blt) || (want_rows > 0 && rows != want_rows)) continue;
+        fdtd::TiledConfig c = batch_cfg(b, blt, rows, pairs32 != 0);
+        if (fdtd::tiled2_batch_supported(c)) cands.push_back(c);
+      }
   if (cands.empty())
     return bfail(b, FDTD_ERR_UNSUPPORTED, "no batched configuration for blt %d, tile_rows %d",
                  want_blt, want_rows);
@@ -1167,7 +1178,7 @@ fdtd_status batch_autotune(fdtd_batch* b, cudaStream_t st) {
     for (const auto& c : cands)
     for (int zl : {0, 64, 32}) {
       b->zlen = zl;
-      if ((s = batch_maps(b, c.rows)) != FDTD_OK) return s;
+      if ((s = batch_maps(b, c)) != FDTD_OK) return s;
       b->ctas = nsm * fdtd::tiled2_batch_ctas_per_sm(c);
       batch_fill_args(b, c, false);
       BCUDA(b, cudaMemcpyAsync(b->d_args, b->h_args, 2 * b->sims.size() * sizeof(fdtd::TiledArgs),
@@ -1282,11 +1293,12 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
   const long long nfull = T / c.blt;
   const int rem = (int)(T % c.blt);
   const int nl = (int)nfull + (rem ? 1 : 0);
-  if ((s = batch_maps(b, c.rows)) != FDTD_OK) return s;
+  if ((s = batch_maps(b, c)) != FDTD_OK) return s;
   if ((s = batch_counters(b, nl)) != FDTD_OK) return s;
   std::pair<int4*, int> tmp;
   if ((s = batch_items(b, c, &tmp)) != FDTD_OK) return s;
-  if (rem && (s = batch_items(b, batch_cfg(b, rem, c.rows), &tmp)) != FDTD_OK) return s;
+  if (rem && (s = batch_items(b, batch_cfg(b, rem, c.rows, c.pairs32), &tmp)) != FDTD_OK)
+    return s;
   batch_fill_args(b, c, true);
 
   auto record = [&](cudaStream_t rs) -> fdtd_status {
@@ -1295,7 +1307,7 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
                              cudaMemcpyHostToDevice, rs));
     BCUDA(b, cudaMemsetAsync(b->d_counters, 0, nl * sizeof(unsigned int), rs));
     for (int k = 0; k < nl; ++k) {
-      const fdtd::TiledConfig ck = (k < nfull) ? c : batch_cfg(b, rem, c.rows);
+      const fdtd::TiledConfig ck = (k < nfull) ? c : batch_cfg(b, rem, c.rows, c.pairs32);
       fdtd_status r = batch_launch(b, ck, k & 1, (long long)k * c.blt, b->d_counters + k, rs);
       if (r != FDTD_OK) return r;
     }
@@ -1339,7 +1351,7 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
   for (fdtd_handle* h : b->sims) {
     h->t += T;
     h->cur ^= (nl & 1);
-    h->last_kernel = FDTD_KERNEL_TILED_W64;
+    h->last_kernel = c.pairs32 ? FDTD_KERNEL_TILED_W32P : FDTD_KERNEL_TILED_W64;
     h->last_launches = nl;
     if ((s = stream_after(b, h->stream, st)) != FDTD_OK) return s;
   }

@@ -63,6 +63,7 @@ struct TiledConfig {
   int min_blocks = 1;  // register cap: CTAs per SM the compiler must fit (x-pair family)
   int storage = 0;     // 0 FP32, 1 FP16, 2 BF16 (x-pair family only for 16-bit)
   int esz = 4;         // bytes per stored field value
+  bool pairs32 = false;  // x-pair kernel with 32-cell rows, two per warp (width must be 32)
 };
 
 // Tile geometry shared by the host (grid size, tensor-map boxes) and the kernel.
@@ -78,6 +79,9 @@ __host__ __device__ constexpr int tiled2_align(int esz) { return 16 / esz; }
 __host__ __device__ constexpr int tiled2_sx(int blt, int esz) {
   return tiled2_align(esz) * ((64 - 2 * blt) / tiled2_align(esz));
 }
+__host__ __device__ constexpr int tiled2_sx_w(int w, int blt, int esz) {
+  return tiled2_align(esz) * ((w - 2 * blt) / tiled2_align(esz));
+}
 __host__ __device__ constexpr int tiled2_xbase(int blt, int esz) {
   return -tiled2_align(esz) * ((blt + tiled2_align(esz) - 1) / tiled2_align(esz));
 }
@@ -87,7 +91,7 @@ bool tiled2_config_supported(const TiledConfig& c);
 dim3 tiled2_grid(const TiledConfig& c, const Grid& g);
 cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& args, const Grid& g,
                           cudaStream_t st);
-// Persistent batch form (ROWS 8 or 16).
+// Persistent batch form.
 bool tiled2_batch_supported(const TiledConfig& c);
 size_t tiled2_batch_smem(const TiledConfig& c);
 int tiled2_batch_ctas_per_sm(const TiledConfig& c);

@@ -1,6 +1,6 @@
 // k_tiled2.cu -- the z-streaming temporally tiled Yee kernel with two cells per thread in x,
 // for one grid (fdtd_tiled2) and for a batch of independent grids in one persistent launch
-// (fdtd_tiled2_batch).
+// (fdtd_tiled2_batch), with 64-cell rows (one per warp) or 32-cell rows (two per warp).
 //
 // Same schedule as k_tiled.cu (TMA plane pipeline, BLT-level (z,t) wavefront, trapezoid tiles in
 // x and y, material map, fused FP64 DFT, bounded waits), but each thread owns an x-pair
@@ -77,15 +77,20 @@ struct Store<__nv_bfloat16> {
   }
 };
 
-template <typename S, int B, int TY>
+// W = 64: one 64-cell row per warp (32 lanes x an x-pair).  W = 32: two 32-cell rows per warp
+// (16 lanes x an x-pair each), so a CTA of the same 16 warps covers a 32 x 32 tile instead of
+// 64 x 16: more of it valid under the trapezoid and a finer x granularity on small grids.
+template <typename S, int B, int TY, int W = 64>
 struct Tiled2 {
   static constexpr int ESZ = (int)sizeof(S);
-  static constexpr int W = 64;                 // cells per warp row
+  static constexpr int LPR = W / 2;            // lanes per tile row
+  static constexpr int THREADS = TY * LPR;
+  static constexpr int MBX = W == 64 ? kMatBoxX2 : kMatBoxX;  // material box width
   static constexpr int PL = W * TY;            // elements of one staged field plane
-  static constexpr int MPL = kMatBoxX2 * TY;   // elements of one staged material plane
+  static constexpr int MPL = MBX * TY;         // elements of one staged material plane
   static constexpr int MPL_S = (MPL * 2 + 127) / 128 * 64;  // its stage stride: 128-byte steps
   static constexpr int NS = ESZ == 4 ? kTiled2Stages : kTiled2Stages + 1;
-  static constexpr int SX = tiled2_sx(B, ESZ);
+  static constexpr int SX = tiled2_sx_w(W, B, ESZ);
   static constexpr int SY = tiled_sy(B, TY);
   static constexpr int XBASE = tiled2_xbase(B, ESZ);
   static constexpr uint32_t STAGE_F_BYTES = 6u * PL * ESZ;
@@ -97,6 +102,7 @@ struct Tiled2 {
   static constexpr size_t OFF_BAR = OFF_E + (size_t)B * 2u * PL * 4u;
   static constexpr size_t SMEM = OFF_BAR + NS * 8u + 128u;  // + alignment slack
   static_assert(SY >= 1, "tile too short for this BLT");
+  static_assert((W == 64 || W == 32) && THREADS % 32 == 0, "warp rows of 64 or 32 cells");
   static_assert(STAGE_M_BYTES % 128 == 0 && (PL * ESZ) % 128 == 0, "stage alignment");
 };
 
@@ -122,10 +128,10 @@ struct Smem {
 // `gbase` counts the pipeline stages this CTA consumed before (mbarrier phases continue across
 // tiles in the persistent form).  Every thread of the CTA calls it; returns false when a
 // bounded wait expired (the CTA must then stop).
-template <typename S, int B, int TY>
+template <typename S, int B, int TY, int W = 64>
 __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz,
                                       const Smem& sm, uint32_t& gbase, long long t_offset) {
-  using K = Tiled2<S, B, TY>;
+  using K = Tiled2<S, B, TY, W>;
   using St = Store<S>;
   S* st_f = reinterpret_cast<S*>(sm.base);
   uint16_t* st_m = reinterpret_cast<uint16_t*>(sm.base + K::OFF_M);
@@ -140,8 +146,9 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   const int ps = z0 - B;
   const int niter = (z1 - z0) + 2 * B;
 
-  const int lx = threadIdx.x, ly = threadIdx.y;
-  const int tid = ly * 32 + lx;
+  const int lx = threadIdx.x % K::LPR;                                   // pair in the row
+  const int ly = threadIdx.y * (32 / K::LPR) + threadIdx.x / K::LPR;     // tile row
+  const int tid = threadIdx.y * 32 + threadIdx.x;
   const int X = bx * K::SX + K::XBASE;  // multiple of 16 bytes of S
   const int Y = by * K::SY - B;
   const int X8 = X & ~7;
@@ -165,7 +172,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   int src_lo = 1 << 30, src_hi = -(1 << 30), mon_lo = 1 << 30, mon_hi = -(1 << 30);
   for (int n = 0; n < a.S.n; ++n) {
     const SourceDev& s = a.S.s[n];
-    if (s.kind == 0 && (s.i < X || s.i >= X + K::W || s.j < Y || s.j >= Y + TY)) continue;
+    if (s.kind == 0 && (s.i < X || s.i >= X + W || s.j < Y || s.j >= Y + TY)) continue;
     src_lo = min(src_lo, s.k);
     src_hi = max(src_hi, s.k + B);
   }
@@ -181,7 +188,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     inv[c] = St::kScaled ? a.inv_scale[c] : 1.0f;
   }
 
-  for (int q = tid; q < (4 + 2 * B) * K::PL; q += 32 * TY) hbuf[q] = 0.0f;
+  for (int q = tid; q < (4 + 2 * B) * K::PL; q += K::THREADS) hbuf[q] = 0.0f;
   __syncthreads();  // zeroed exchange planes; the previous tile's stages are all consumed
 
   auto issue = [&](int it_) {
@@ -210,10 +217,10 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
 #pragma unroll
   for (int s = 0; s <= B; ++s) mq[s] = 0;
 
-  const int o = ly * K::W + cx0;
-  const int oym = (ly > 0 ? ly - 1 : 0) * K::W + cx0;
-  const int oyp = (ly < TY - 1 ? ly + 1 : TY - 1) * K::W + cx0;
-  const int om = ly * kMatBoxX2 + cx0 + (X - X8);  // even: a 4-byte aligned id pair
+  const int o = ly * W + cx0;
+  const int oym = (ly > 0 ? ly - 1 : 0) * W + cx0;
+  const int oyp = (ly < TY - 1 ? ly + 1 : TY - 1) * W + cx0;
+  const int om = ly * K::MBX + cx0 + (X - X8);  // even: a 4-byte aligned id pair
   const float dx = a.dx;
   const long long pitch = g.pitch, plane = g.plane;
   S* const* dst = reinterpret_cast<S* const*>(a.dst.f);
@@ -255,8 +262,8 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
       const long long t = a.t0 + t_offset + (s - 1);
       // ---------------- E^s(e)
       // x-1 neighbour: odd cell of lane-1 for the even cell, own even cell for the odd cell
-      const float hz_xm = __shfl_up_sync(kFull, Hc[2].b, 1);
-      const float hy_xm = __shfl_up_sync(kFull, Hc[1].b, 1);
+      const float hz_xm = __shfl_up_sync(kFull, Hc[2].b, 1, K::LPR);
+      const float hy_xm = __shfl_up_sync(kFull, Hc[1].b, 1, K::LPR);
       Pair cxp, cyp, czp;
       cxp.a = sub(sub(Hc[2].a, hz_ym.x), sub(Hc[1].a, Hp[s - 1][1].a));
       cxp.b = sub(sub(Hc[2].b, hz_ym.y), sub(Hc[1].b, Hp[s - 1][1].b));
@@ -292,8 +299,8 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
       }
       // ---------------- H^s(e-1)
       // x+1 neighbour: own odd cell for the even cell, even cell of lane+1 for the odd cell
-      const float ez_xp = __shfl_down_sync(kFull, Ep[s][2].a, 1);
-      const float ey_xp = __shfl_down_sync(kFull, Ep[s][1].a, 1);
+      const float ez_xp = __shfl_down_sync(kFull, Ep[s][2].a, 1, K::LPR);
+      const float ey_xp = __shfl_down_sync(kFull, Ep[s][1].a, 1, K::LPR);
       float* eb = ebuf + (s - 1) * 2 * K::PL;
       const float2 ex_yp = ldf2(eb + oyp), ez_yp = ldf2(eb + K::PL + oyp);
       cxp.a = sub(sub(En[1].a, Ep[s][1].a), sub(ez_yp.x, Ep[s][2].a));
@@ -429,9 +436,9 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   return true;
 }
 
-template <typename S, int B, int TY>
+template <typename S, int B, int TY, int W = 64>
 __device__ __forceinline__ Smem setup_smem(unsigned char* smem_raw, int* s_abort) {
-  using K = Tiled2<S, B, TY>;
+  using K = Tiled2<S, B, TY, W>;
   unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   Smem sm{base, reinterpret_cast<uint64_t*>(base + K::OFF_BAR), s_abort};
   if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -444,23 +451,23 @@ __device__ __forceinline__ Smem setup_smem(unsigned char* smem_raw, int* s_abort
 
 // One grid: one tile per CTA.  MINB > 1 caps registers so that MINB CTAs fit on an SM (more
 // warps to hide latency, at the cost of some spilled state); the autotuner decides.
-template <typename S, int B, int TY, int MINB>
-__global__ void __launch_bounds__(32 * TY, MINB)
+template <typename S, int B, int TY, int MINB, int W = 64>
+__global__ void __launch_bounds__(TY * W / 2, MINB)
     fdtd_tiled2(const __grid_constant__ TiledArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_abort;
-  const Smem sm = setup_smem<S, B, TY>(smem_raw, &s_abort);
+  const Smem sm = setup_smem<S, B, TY, W>(smem_raw, &s_abort);
   uint32_t gbase = 0;
-  (void)march<S, B, TY>(a, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, sm, gbase, 0);
+  (void)march<S, B, TY, W>(a, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, sm, gbase, 0);
 }
 
 // A batch of independent grids: persistent CTAs pull (grid, tile) work items from a queue.
-template <typename S, int B, int TY>
-__global__ void __launch_bounds__(32 * TY, 1) fdtd_tiled2_batch(const BatchArgs b) {
+template <typename S, int B, int TY, int W = 64>
+__global__ void __launch_bounds__(TY * W / 2, 1) fdtd_tiled2_batch(const BatchArgs b) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_abort;
   __shared__ int s_item;
-  const Smem sm = setup_smem<S, B, TY>(smem_raw, &s_abort);
+  const Smem sm = setup_smem<S, B, TY, W>(smem_raw, &s_abort);
   const int tid = threadIdx.y * 32 + threadIdx.x;
   uint32_t gbase = 0;
   while (true) {
@@ -471,28 +478,66 @@ __global__ void __launch_bounds__(32 * TY, 1) fdtd_tiled2_batch(const BatchArgs 
     if (item >= b.nitems) break;
     const int4 w = b.items[item];  // {grid, bx, by, bz}
     const TiledArgs& a = b.grids[b.flip * b.ngrids + w.x];
-    if (!march<S, B, TY>(a, w.y, w.z, w.w, sm, gbase, b.t_offset)) break;
+    if (!march<S, B, TY, W>(a, w.y, w.z, w.w, sm, gbase, b.t_offset)) break;
   }
 }
 
-template <typename S, int B, int TY, int MINB>
+template <typename S, int B, int TY, int MINB, int W = 64>
 cudaError_t launch_one2(const TiledArgs& a, dim3 grid, cudaStream_t st) {
-  using K = Tiled2<S, B, TY>;
-  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2<S, B, TY, MINB>,
+  using K = Tiled2<S, B, TY, W>;
+  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2<S, B, TY, MINB, W>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
   if (e != cudaSuccess) return e;
-  fdtd_tiled2<S, B, TY, MINB><<<grid, dim3(32, TY), K::SMEM, st>>>(a);
+  fdtd_tiled2<S, B, TY, MINB, W><<<grid, dim3(32, K::THREADS / 32), K::SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
-template <typename S, int B, int TY>
+template <typename S, int B, int TY, int W = 64>
 cudaError_t launch_batch_one(const BatchArgs& b, int ctas, cudaStream_t st) {
-  using K = Tiled2<S, B, TY>;
-  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2_batch<S, B, TY>,
+  using K = Tiled2<S, B, TY, W>;
+  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2_batch<S, B, TY, W>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
   if (e != cudaSuccess) return e;
-  fdtd_tiled2_batch<S, B, TY><<<ctas, dim3(32, TY), K::SMEM, st>>>(b);
+  fdtd_tiled2_batch<S, B, TY, W><<<ctas, dim3(32, K::THREADS / 32), K::SMEM, st>>>(b);
   return cudaGetLastError();
+}
+
+// 32-wide rows (two per warp), FP32: 32 rows (16 warps, BLT 1-3) or 48 rows (24 warps, BLT 1-2).
+cudaError_t launch_pairs32(int blt, int rows, const TiledArgs& a, dim3 grid, cudaStream_t st) {
+  if (rows == 32) {
+    switch (blt) {
+      case 1: return launch_one2<float, 1, 32, 1, 32>(a, grid, st);
+      case 2: return launch_one2<float, 2, 32, 1, 32>(a, grid, st);
+      case 3: return launch_one2<float, 3, 32, 1, 32>(a, grid, st);
+      default: break;
+    }
+  } else if (rows == 48) {
+    switch (blt) {
+      case 1: return launch_one2<float, 1, 48, 1, 32>(a, grid, st);
+      case 2: return launch_one2<float, 2, 48, 1, 32>(a, grid, st);
+      default: break;
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_batch_pairs32(int blt, int rows, const BatchArgs& b, int ctas,
+                                 cudaStream_t st) {
+  if (rows == 32) {
+    switch (blt) {
+      case 1: return launch_batch_one<float, 1, 32, 32>(b, ctas, st);
+      case 2: return launch_batch_one<float, 2, 32, 32>(b, ctas, st);
+      case 3: return launch_batch_one<float, 3, 32, 32>(b, ctas, st);
+      default: break;
+    }
+  } else if (rows == 48) {
+    switch (blt) {
+      case 1: return launch_batch_one<float, 1, 48, 32>(b, ctas, st);
+      case 2: return launch_batch_one<float, 2, 48, 32>(b, ctas, st);
+      default: break;
+    }
+  }
+  return cudaErrorInvalidValue;
 }
 
 template <typename S, int TY>
@@ -574,20 +619,26 @@ cudaError_t launch_batch_type(const TiledConfig& c, const BatchArgs& b, int ctas
   return cudaErrorInvalidValue;
 }
 
-template <typename S, int B, int TY>
+template <typename S, int B, int TY, int W = 64>
 size_t smem_of() {
-  return Tiled2<S, B, TY>::SMEM;
+  return Tiled2<S, B, TY, W>::SMEM;
 }
 
-template <typename S, int B, int TY>
+template <typename S, int B, int TY, int W = 64>
 int occupancy_of() {
+  using K = Tiled2<S, B, TY, W>;
   int n = 0;
-  cudaFuncSetAttribute(fdtd_tiled2_batch<S, B, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)Tiled2<S, B, TY>::SMEM);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fdtd_tiled2_batch<S, B, TY>, 32 * TY,
-                                                    Tiled2<S, B, TY>::SMEM) != cudaSuccess)
+  cudaFuncSetAttribute(fdtd_tiled2_batch<S, B, TY, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)K::SMEM);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fdtd_tiled2_batch<S, B, TY, W>, K::THREADS,
+                                                    K::SMEM) != cudaSuccess)
     return 1;
   return n > 0 ? n : 1;
+}
+
+bool pairs32_supported(const TiledConfig& c) {
+  return c.esz == 4 && c.width == 32 && c.min_blocks == 1 &&
+         ((c.rows == 32 && c.blt >= 1 && c.blt <= 3) || (c.rows == 48 && c.blt >= 1 && c.blt <= 2));
 }
 
 template <typename S>
@@ -625,6 +676,7 @@ int batch_occupancy_type(const TiledConfig& c) {
 }  // namespace
 
 bool tiled2_config_supported(const TiledConfig& c) {
+  if (c.pairs32) return pairs32_supported(c) && c.z_chunks >= 1;
   if (c.esz != 4 && c.esz != 2) return false;
   if (c.rows != 8 && c.rows != 16 && c.rows != 20 && c.rows != 24 && c.rows != 32) return false;
   if (c.rows > 16 && c.esz != 4) return false;
@@ -639,6 +691,7 @@ bool tiled2_config_supported(const TiledConfig& c) {
 }
 
 bool tiled2_batch_supported(const TiledConfig& c) {
+  if (c.pairs32) return pairs32_supported(c);
   if (c.esz != 4 && c.esz != 2) return false;
   if (c.rows == 16) return c.blt >= 1 && c.blt <= 4;
   if (c.rows == 8) return c.blt >= 1 && c.blt <= 3;
@@ -648,7 +701,7 @@ bool tiled2_batch_supported(const TiledConfig& c) {
 }
 
 dim3 tiled2_grid(const TiledConfig& c, const Grid& g) {
-  const int sx = tiled2_sx(c.blt, c.esz), sy = tiled_sy(c.blt, c.rows);
+  const int sx = tiled2_sx_w(c.pairs32 ? 32 : 64, c.blt, c.esz), sy = tiled_sy(c.blt, c.rows);
   const int first = tiled2_xbase(c.blt, c.esz) + c.blt;
   const int ntx = (g.nx - first + sx - 1) / sx;
   const int nty = (g.ny + sy - 1) / sy;
@@ -659,6 +712,21 @@ dim3 tiled2_grid(const TiledConfig& c, const Grid& g) {
 
 size_t tiled2_batch_smem(const TiledConfig& c) {
   const bool h = c.esz == 2;
+  if (c.pairs32) {
+    if (c.rows == 32) {
+      switch (c.blt) {
+        case 1: return smem_of<float, 1, 32, 32>();
+        case 2: return smem_of<float, 2, 32, 32>();
+        case 3: return smem_of<float, 3, 32, 32>();
+      }
+    } else if (c.rows == 48) {
+      switch (c.blt) {
+        case 1: return smem_of<float, 1, 48, 32>();
+        case 2: return smem_of<float, 2, 48, 32>();
+      }
+    }
+    return 0;
+  }
   if (c.rows == 16) {
     switch (c.blt) {
       case 1: return h ? smem_of<__half, 1, 16>() : smem_of<float, 1, 16>();
@@ -688,6 +756,21 @@ size_t tiled2_batch_smem(const TiledConfig& c) {
 }
 
 int tiled2_batch_ctas_per_sm(const TiledConfig& c) {
+  if (c.pairs32) {
+    if (c.rows == 32) {
+      switch (c.blt) {
+        case 1: return occupancy_of<float, 1, 32, 32>();
+        case 2: return occupancy_of<float, 2, 32, 32>();
+        case 3: return occupancy_of<float, 3, 32, 32>();
+      }
+    } else if (c.rows == 48) {
+      switch (c.blt) {
+        case 1: return occupancy_of<float, 1, 48, 32>();
+        case 2: return occupancy_of<float, 2, 48, 32>();
+      }
+    }
+    return 1;
+  }
   switch (c.storage) {
     case 0: return batch_occupancy_type<float>(c);
     case 1: return batch_occupancy_type<__half>(c);
@@ -700,6 +783,7 @@ cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& a, const Grid& 
                           cudaStream_t st) {
   if (!tiled2_config_supported(c)) return cudaErrorInvalidValue;
   const dim3 grid = tiled2_grid(c, g);
+  if (c.pairs32) return launch_pairs32(c.blt, c.rows, a, grid, st);
   switch (c.storage) {
     case 0: return launch_type2<float>(c, a, grid, st);
     case 1: return launch_type2<__half>(c, a, grid, st);
@@ -711,6 +795,7 @@ cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& a, const Grid& 
 cudaError_t launch_tiled2_batch(const TiledConfig& c, const BatchArgs& b, int ctas,
                                 cudaStream_t st) {
   if (!tiled2_batch_supported(c)) return cudaErrorInvalidValue;
+  if (c.pairs32) return launch_batch_pairs32(c.blt, c.rows, b, ctas, st);
   switch (c.storage) {
     case 0: return launch_batch_type<float>(c, b, ctas, st);
     case 1: return launch_batch_type<__half>(c, b, ctas, st);

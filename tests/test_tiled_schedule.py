@@ -25,7 +25,8 @@ def bits_equal(a, b):
                           np.asarray(b, np.float32).view(np.uint32))
 
 
-CONFIGS = [(b, r, z, 32) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)), (32, (1, 4, 6)))
+CONFIGS = [(b, r, z, 32) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)), (32, (1, 2, 3, 4, 6)),
+                                       (48, (1, 2)))
            for b in bs for z in (1, 3)]
 CONFIGS += [(b, r, z, 64) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4)), (20, (1, 2, 3)),
                                         (24, (1, 2)), (32, (1, 2)))
@@ -78,7 +79,7 @@ def test_schedule_plane_source_and_monitors(blt, rows, zc, width):
 def test_output_windows_tile_the_grid():
     """Every cell is written exactly once per pass and nothing outside the grid."""
     for width, blt, rows in [(w, b, r) for w in (32, 64) for b in range(1, 7)
-                             for r in (8, 16, 20, 24, 32)]:
+                             for r in (8, 16, 20, 24, 32, 48)]:
         if rows - 2 * blt < 1:
             continue
         for shape in ((3, 3, 3), (33, 17, 9), (100, 61, 5)):
