@@ -275,8 +275,8 @@ std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
   std::vector<int> fams = {0, 1, 2};
   const bool half = h->esz == 2;
   if (half) {
-    fams = {1};
-    rows_l = {8, 16};
+    fams = {1, 2};
+    rows_l = {8, 16, 32, 48};
   }
   if (h->desc.blt > 0) blts = {h->desc.blt};
   if (h->desc.tile_rows > 0) rows_l = {h->desc.tile_rows};
@@ -507,8 +507,7 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
   if (d->kernel < FDTD_KERNEL_AUTO || d->kernel > FDTD_KERNEL_TILED_W32P)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "unknown kernel %d", d->kernel);
   if ((d->storage == FDTD_STORE_F16 || d->storage == FDTD_STORE_BF16) &&
-      (d->kernel == FDTD_KERNEL_NAIVE || d->kernel == FDTD_KERNEL_TILED_W32 ||
-       d->kernel == FDTD_KERNEL_TILED_W32P))
+      (d->kernel == FDTD_KERNEL_NAIVE || d->kernel == FDTD_KERNEL_TILED_W32))
     return fail(nullptr, FDTD_ERR_UNSUPPORTED,
                 "16-bit field storage runs the tiled x-pair kernel only");
   if (d->storage == FDTD_STORE_F64 && d->kernel != FDTD_KERNEL_AUTO &&
@@ -1055,13 +1054,18 @@ fdtd::TiledConfig batch_cfg(const fdtd_batch* b, int blt, int rows, bool pairs32
   return c;
 }
 
+// Key of a batch's work-item list: z-chunk length and the tile configuration.
+int items_key(int zlen, const fdtd::TiledConfig& c) {
+  return ((zlen * 10 + c.blt) * 100 + c.rows) * 2 + (c.pairs32 ? 1 : 0);
+}
+
 // z-chunks of one simulation for a target chunk length (0: one chunk per column).
 int sim_chunks(const Grid& g, int zlen) { return zlen <= 0 ? 1 : std::max(1, (g.nz + zlen - 1) / zlen); }
 
 // Work items of one (BLT, rows, chunk length): every z-chunk of every tile column of every
 // simulation, longest z-march first so the queue's tail is short.
 fdtd_status batch_items(fdtd_batch* b, const fdtd::TiledConfig& c, std::pair<int4*, int>* out) {
-  const int key = ((b->zlen * 10 + c.blt) * 100 + c.rows) * 2 + (c.pairs32 ? 1 : 0);
+  const int key = items_key(b->zlen, c);
   auto it = b->items.find(key);
   if (it != b->items.end()) {
     *out = it->second;
@@ -1364,7 +1368,7 @@ fdtd_status fdtd_batch_get_config(const fdtd_batch* b, int32_t* out6) {
   out6[0] = b->cfg.blt;
   out6[1] = b->cfg.rows;
   out6[2] = b->ctas;
-  auto it = b->items.find((b->zlen * 10 + b->cfg.blt) * 100 + b->cfg.rows);
+  auto it = b->items.find(items_key(b->zlen, b->cfg));
   out6[3] = it == b->items.end() ? 0 : it->second.second;
   out6[4] = b->last_launches;
   out6[5] = b->last_graph;

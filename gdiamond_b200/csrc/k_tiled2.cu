@@ -502,38 +502,40 @@ cudaError_t launch_batch_one(const BatchArgs& b, int ctas, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// 32-wide rows (two per warp), FP32: 32 rows (16 warps, BLT 1-3) or 48 rows (24 warps, BLT 1-2).
+// 32-wide rows (two per warp): 32 rows (16 warps, BLT 1-3) or 48 rows (24 warps, BLT 1-2).
+template <typename S>
 cudaError_t launch_pairs32(int blt, int rows, const TiledArgs& a, dim3 grid, cudaStream_t st) {
   if (rows == 32) {
     switch (blt) {
-      case 1: return launch_one2<float, 1, 32, 1, 32>(a, grid, st);
-      case 2: return launch_one2<float, 2, 32, 1, 32>(a, grid, st);
-      case 3: return launch_one2<float, 3, 32, 1, 32>(a, grid, st);
+      case 1: return launch_one2<S, 1, 32, 1, 32>(a, grid, st);
+      case 2: return launch_one2<S, 2, 32, 1, 32>(a, grid, st);
+      case 3: return launch_one2<S, 3, 32, 1, 32>(a, grid, st);
       default: break;
     }
   } else if (rows == 48) {
     switch (blt) {
-      case 1: return launch_one2<float, 1, 48, 1, 32>(a, grid, st);
-      case 2: return launch_one2<float, 2, 48, 1, 32>(a, grid, st);
+      case 1: return launch_one2<S, 1, 48, 1, 32>(a, grid, st);
+      case 2: return launch_one2<S, 2, 48, 1, 32>(a, grid, st);
       default: break;
     }
   }
   return cudaErrorInvalidValue;
 }
 
+template <typename S>
 cudaError_t launch_batch_pairs32(int blt, int rows, const BatchArgs& b, int ctas,
                                  cudaStream_t st) {
   if (rows == 32) {
     switch (blt) {
-      case 1: return launch_batch_one<float, 1, 32, 32>(b, ctas, st);
-      case 2: return launch_batch_one<float, 2, 32, 32>(b, ctas, st);
-      case 3: return launch_batch_one<float, 3, 32, 32>(b, ctas, st);
+      case 1: return launch_batch_one<S, 1, 32, 32>(b, ctas, st);
+      case 2: return launch_batch_one<S, 2, 32, 32>(b, ctas, st);
+      case 3: return launch_batch_one<S, 3, 32, 32>(b, ctas, st);
       default: break;
     }
   } else if (rows == 48) {
     switch (blt) {
-      case 1: return launch_batch_one<float, 1, 48, 32>(b, ctas, st);
-      case 2: return launch_batch_one<float, 2, 48, 32>(b, ctas, st);
+      case 1: return launch_batch_one<S, 1, 48, 32>(b, ctas, st);
+      case 2: return launch_batch_one<S, 2, 48, 32>(b, ctas, st);
       default: break;
     }
   }
@@ -637,8 +639,42 @@ int occupancy_of() {
 }
 
 bool pairs32_supported(const TiledConfig& c) {
-  return c.esz == 4 && c.width == 32 && c.min_blocks == 1 &&
+  return (c.esz == 4 || c.esz == 2) && c.width == 32 && c.min_blocks == 1 &&
          ((c.rows == 32 && c.blt >= 1 && c.blt <= 3) || (c.rows == 48 && c.blt >= 1 && c.blt <= 2));
+}
+
+template <typename S>
+size_t pairs32_smem(const TiledConfig& c) {
+  if (c.rows == 32) {
+    switch (c.blt) {
+      case 1: return smem_of<S, 1, 32, 32>();
+      case 2: return smem_of<S, 2, 32, 32>();
+      case 3: return smem_of<S, 3, 32, 32>();
+    }
+  } else if (c.rows == 48) {
+    switch (c.blt) {
+      case 1: return smem_of<S, 1, 48, 32>();
+      case 2: return smem_of<S, 2, 48, 32>();
+    }
+  }
+  return 0;
+}
+
+template <typename S>
+int pairs32_occupancy(const TiledConfig& c) {
+  if (c.rows == 32) {
+    switch (c.blt) {
+      case 1: return occupancy_of<S, 1, 32, 32>();
+      case 2: return occupancy_of<S, 2, 32, 32>();
+      case 3: return occupancy_of<S, 3, 32, 32>();
+    }
+  } else if (c.rows == 48) {
+    switch (c.blt) {
+      case 1: return occupancy_of<S, 1, 48, 32>();
+      case 2: return occupancy_of<S, 2, 48, 32>();
+    }
+  }
+  return 1;
 }
 
 template <typename S>
@@ -713,17 +749,10 @@ dim3 tiled2_grid(const TiledConfig& c, const Grid& g) {
 size_t tiled2_batch_smem(const TiledConfig& c) {
   const bool h = c.esz == 2;
   if (c.pairs32) {
-    if (c.rows == 32) {
-      switch (c.blt) {
-        case 1: return smem_of<float, 1, 32, 32>();
-        case 2: return smem_of<float, 2, 32, 32>();
-        case 3: return smem_of<float, 3, 32, 32>();
-      }
-    } else if (c.rows == 48) {
-      switch (c.blt) {
-        case 1: return smem_of<float, 1, 48, 32>();
-        case 2: return smem_of<float, 2, 48, 32>();
-      }
+    switch (c.storage) {
+      case 0: return pairs32_smem<float>(c);
+      case 1: return pairs32_smem<__half>(c);
+      case 2: return pairs32_smem<__nv_bfloat16>(c);
     }
     return 0;
   }
@@ -757,17 +786,10 @@ size_t tiled2_batch_smem(const TiledConfig& c) {
 
 int tiled2_batch_ctas_per_sm(const TiledConfig& c) {
   if (c.pairs32) {
-    if (c.rows == 32) {
-      switch (c.blt) {
-        case 1: return occupancy_of<float, 1, 32, 32>();
-        case 2: return occupancy_of<float, 2, 32, 32>();
-        case 3: return occupancy_of<float, 3, 32, 32>();
-      }
-    } else if (c.rows == 48) {
-      switch (c.blt) {
-        case 1: return occupancy_of<float, 1, 48, 32>();
-        case 2: return occupancy_of<float, 2, 48, 32>();
-      }
+    switch (c.storage) {
+      case 0: return pairs32_occupancy<float>(c);
+      case 1: return pairs32_occupancy<__half>(c);
+      case 2: return pairs32_occupancy<__nv_bfloat16>(c);
     }
     return 1;
   }
@@ -783,7 +805,14 @@ cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& a, const Grid& 
                           cudaStream_t st) {
   if (!tiled2_config_supported(c)) return cudaErrorInvalidValue;
   const dim3 grid = tiled2_grid(c, g);
-  if (c.pairs32) return launch_pairs32(c.blt, c.rows, a, grid, st);
+  if (c.pairs32) {
+    switch (c.storage) {
+      case 0: return launch_pairs32<float>(c.blt, c.rows, a, grid, st);
+      case 1: return launch_pairs32<__half>(c.blt, c.rows, a, grid, st);
+      case 2: return launch_pairs32<__nv_bfloat16>(c.blt, c.rows, a, grid, st);
+      default: return cudaErrorInvalidValue;
+    }
+  }
   switch (c.storage) {
     case 0: return launch_type2<float>(c, a, grid, st);
     case 1: return launch_type2<__half>(c, a, grid, st);
@@ -795,7 +824,14 @@ cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& a, const Grid& 
 cudaError_t launch_tiled2_batch(const TiledConfig& c, const BatchArgs& b, int ctas,
                                 cudaStream_t st) {
   if (!tiled2_batch_supported(c)) return cudaErrorInvalidValue;
-  if (c.pairs32) return launch_batch_pairs32(c.blt, c.rows, b, ctas, st);
+  if (c.pairs32) {
+    switch (c.storage) {
+      case 0: return launch_batch_pairs32<float>(c.blt, c.rows, b, ctas, st);
+      case 1: return launch_batch_pairs32<__half>(c.blt, c.rows, b, ctas, st);
+      case 2: return launch_batch_pairs32<__nv_bfloat16>(c.blt, c.rows, b, ctas, st);
+      default: return cudaErrorInvalidValue;
+    }
+  }
   switch (c.storage) {
     case 0: return launch_batch_type<float>(c, b, ctas, st);
     case 1: return launch_batch_type<__half>(c, b, ctas, st);

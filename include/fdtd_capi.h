@@ -66,7 +66,7 @@ typedef enum fdtd_kernel {
                                  the autotuner picks the family below */
   FDTD_KERNEL_TILED_W32 = 3,  /* tiled, one cell per thread (32-wide warp rows) */
   FDTD_KERNEL_TILED_W64 = 4,  /* tiled, an x-pair of cells per thread (64-wide warp rows) */
-  FDTD_KERNEL_TILED_W32P = 5  /* tiled, an x-pair per thread, two 32-wide rows per warp (FP32) */
+  FDTD_KERNEL_TILED_W32P = 5  /* tiled, an x-pair per thread, two 32-wide rows per warp */
 } fdtd_kernel;
 
 /* Field storage in HBM.  F32/F16/BF16 update in FP32 arithmetic; F16/BF16 store each
@@ -87,8 +87,7 @@ typedef struct fdtd_desc {
   int32_t storage;      /* fdtd_storage */
   int32_t kernel;       /* fdtd_kernel */
   int32_t blt;          /* time steps per tiled launch; 0 = autotuned */
-  int32_t tile_rows;    /* tiled-kernel rows per tile (8, 16, 20, 24, 32 or 48; 20, 24 and 48
-                           for FP32 x-pair kernels only); 0 = autotuned */
+  int32_t tile_rows;    /* tiled-kernel rows per tile (8, 16, 20, 24, 32 or 48); 0 = autotuned */
   int32_t z_chunks;     /* tiled-kernel z-chunks per column; 0 = autotuned */
   int32_t min_blocks;   /* tiled x-pair family: CTAs per SM the registers must allow (1, 2 or
                            4); 0 = autotuned */

@@ -98,6 +98,32 @@ def test_16bit_storage_matches_rounded_oracle(storage, blt, rows):
     assert np.array_equal(re, omons[0].re) and np.array_equal(im, omons[0].im)
 
 
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("blt,rows", [(1, 48), (2, 32), (2, 48), (3, 32)])
+def test_16bit_pairs32_matches_rounded_oracle(storage, blt, rows):
+    """The x-pair kernel with 32-cell rows (two per warp) and 16-bit storage."""
+    shape, T = (70, 41, 33), 14
+    coefs, src, mons = setup(shape, T, 5)
+    scales = [8.0, 8.0, 8.0, 2.0, 2.0, 0.5]
+    omons = [oracle.Monitor(m["component"], m["k"], m["freqs"], m["scale"]) for m in mons]
+    F_ref = oracle_stored(shape, coefs, T, blt, storage, scales, [osrc(s) for s in src], omons)
+    sim = gd.Simulation(*shape, storage=storage, kernel="tiled_w32p", blt=blt, tile_rows=rows)
+    sim.set_storage_scale(scales)
+    sim.set_coefficients(coefs)
+    sim.set_sources(src)
+    mid = sim.add_dft_monitor(mons[0]["component"], mons[0]["k"], mons[0]["freqs"])
+    sim.step(T)
+    sim.sync()
+    F = sim.fields()
+    re, im = sim.get_dft(mid)
+    cfg = sim.config()
+    sim.close()
+    assert (cfg["width"], cfg["pairs"], cfg["blt"], cfg["tile_rows"]) == (32, True, blt, rows)
+    for c in range(6):
+        assert bits_equal(F[c], F_ref[c]), oracle.COMPONENTS[c]
+    assert np.array_equal(re, omons[0].re) and np.array_equal(im, omons[0].im)
+
+
 def test_16bit_rejects_naive_and_accepts_power_of_two_scales():
     with pytest.raises(gd.FdtdError):
         gd.Simulation(20, 20, 20, storage="f16", kernel="naive")
