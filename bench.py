@@ -411,7 +411,8 @@ def fp16_scales(probe, ncell, T, every=1, headroom=2048.0):
 def run_mixed(args):
     """Mixed-precision FDTD: 512x512x384 grid, 200 seeded dielectric spheres, Gaussian Jz at the
     centre, FP64 running DFT of Ez at 16 frequencies on the planes z=96 and z=288, 2000 steps.
-    FP32, BF16 and FP16 field storage against an FP64 run of the same grid."""
+    FP32, BF16, FP16 and F16E (FP16 E, FP32 H) field storage against an FP64 run of the same
+    grid."""
     import torch
     import gdiamond_b200 as gd
     from gdiamond_b200 import workloads as W
@@ -444,7 +445,8 @@ def run_mixed(args):
     ref.close()
     res["f64"] = {"gcells": ncell * T / t64 / 1e9, "seconds": t64}
     f16_scales = fp16_scales(make("f32"), ncell, min(T, 400))
-    for storage, scales in (("f32", None), ("bf16", None), ("f16", f16_scales)):
+    for storage, scales in (("f32", None), ("bf16", None), ("f16", f16_scales),
+                            ("f16e", f16_scales)):
         sim = make(storage, scales)
         sim.step(2 * 4)  # autotune + warm-up outside the timed run
         sim.reset()
@@ -523,7 +525,7 @@ def run_batched(args):
     f16 = fp16_scales(make((shape0, np.ones(int(np.prod(shape0)), np.float32), pos0), "f32"),
                       int(np.prod(shape0)), min(T, 300))
     for storage in args.batch_storage.split(","):
-        scales = f16 if storage == "f16" else None
+        scales = f16 if storage in ("f16", "f16e") else None  # f16e scales E only
         sims = [make(sp, storage, scales, blt=args.blt) for sp in specs]
         batch = gd.Batch(sims)
         batch.step(4)  # batch autotune outside the timed region
@@ -735,7 +737,7 @@ def main():
                     help="plain: the benchmark line; mixed / batched: the precision and "
                          "batching configurations (separate JSON lines)")
     ap.add_argument("--sims", type=int, default=64, help="batched workload: simulations")
-    ap.add_argument("--batch-storage", default="bf16,f16,f32",
+    ap.add_argument("--batch-storage", default="bf16,f16,f16e,f32",
                     help="batched workload: storages of the batched runs")
     ap.add_argument("--designs", type=int, default=1 << 20, help="mlp: designs per inference")
     ap.add_argument("--train-epochs", type=int, default=10, help="mlp: timed training epochs")

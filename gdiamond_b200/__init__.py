@@ -23,7 +23,7 @@ COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 SOURCE_COMPONENTS = ("Jx", "Jy", "Jz", "Mx", "My", "Mz")
 COEFFS = ("Cax", "Cay", "Caz", "Cbx", "Cby", "Cbz", "Dax", "Day", "Daz", "Dbx", "Dby", "Dbz")
 KERNELS = {"auto": 0, "naive": 1, "tiled": 2, "tiled_w32": 3, "tiled_w64": 4, "tiled_w32p": 5}
-STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3}
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f64": 3, "f16e": 4}  # f16e: FP16 E, FP32 H
 SRC_POINT, SRC_PLANE_Z = 0, 1
 
 # Every symbol declared in include/fdtd_capi.h.
@@ -40,7 +40,7 @@ EXPORTS = (
     "fdtd_mlp_get_params", "fdtd_mlp_set_params", "fdtd_mlp_set_data", "fdtd_mlp_grad",
     "fdtd_mlp_train", "fdtd_mlp_predict", "fdtd_mlp_predict_device", "fdtd_get_dft_device",
     "fdtd_mlp_set_gemm", "fdtd_get_planes_device", "fdtd_set_planes_device",
-    "fdtd_storage_bytes", "fdtd_set_step", "fdtd_set_dft",
+    "fdtd_storage_bytes", "fdtd_set_step", "fdtd_set_dft", "fdtd_component_bytes",
 )
 
 
@@ -100,6 +100,7 @@ def library():
             "fdtd_get_planes_device": ([V, C.c_int32, C.c_int64, C.c_int64, V, V], C.c_int),
             "fdtd_set_planes_device": ([V, C.c_int32, C.c_int64, C.c_int64, V, V], C.c_int),
             "fdtd_storage_bytes": ([V, P(C.c_int32)], C.c_int),
+            "fdtd_component_bytes": ([V, C.c_int32, P(C.c_int32)], C.c_int),
             "fdtd_set_step": ([V, C.c_int64], C.c_int),
             "fdtd_set_dft": ([V, C.c_int32, P(C.c_double), P(C.c_double)], C.c_int),
             "fdtd_batch_create": ([P(V), C.c_int32, P(V)], C.c_int),
@@ -342,6 +343,13 @@ class Simulation:
         self._check(self._L.fdtd_storage_bytes(self._h, C.byref(n)))
         return n.value
 
+    def component_bytes(self, component):
+        """Bytes per stored value of one component (differs between E and H for f16e)."""
+        comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
+        n = C.c_int32()
+        self._check(self._L.fdtd_component_bytes(self._h, comp, C.byref(n)))
+        return n.value
+
     def get_planes_device(self, component, k0, nk, ptr, stream=None):
         """Raw copy of z-planes [k0, k0+nk) of a component (current set) to a device buffer."""
         comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
@@ -370,12 +378,12 @@ class Simulation:
         import torch
         self.sync()
         nx, ny, nz = self.shape
-        esz = self.storage_bytes()
-        raw = {2: torch.int16, 4: torch.int32, 8: torch.int64}[esz]
+        esz = [self.component_bytes(c) for c in range(6)]
         dev = torch.device("cuda", self._device)
-        buf = torch.empty((nz, ny, nx), dtype=raw, device=dev)
         fields = []
         for c in range(6):
+            raw = {2: torch.int16, 4: torch.int32, 8: torch.int64}[esz[c]]
+            buf = torch.empty((nz, ny, nx), dtype=raw, device=dev)
             self.get_planes_device(c, 0, nz, buf.data_ptr())
             self.sync()
             fields.append(buf.cpu().numpy().copy())
@@ -384,7 +392,8 @@ class Simulation:
 
     def restore(self, ckpt):
         import torch
-        if tuple(ckpt["shape"]) != self.shape or ckpt["esz"] != self.storage_bytes():
+        if (tuple(ckpt["shape"]) != self.shape
+                or list(ckpt["esz"]) != [self.component_bytes(c) for c in range(6)]):
             raise ValueError("checkpoint of another shape or storage")
         if len(ckpt["dft"]) != self.n_monitors:
             raise ValueError("checkpoint with another set of monitors")

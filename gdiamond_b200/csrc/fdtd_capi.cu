@@ -62,7 +62,7 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
 
 // Process-wide autotuning cache keyed by grid shape.
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int>, fdtd::TiledConfig> g_tune_cache;
+std::map<std::tuple<int, int, int, long long>, fdtd::TiledConfig> g_tune_cache;
 
 }  // namespace
 
@@ -94,7 +94,7 @@ struct fdtd_handle {
   int maps_key = 0;  // width * 1000 + rows of the encoded boxes
   int last_kernel = 0, last_launches = 0;
   int storage = FDTD_STORE_F32;
-  int esz = 4;     // bytes per stored field value
+  int esz = 4;     // bytes per stored field value (F16E: the FP16 E components')
   int nsets = 2;   // field sets (1 for FP64: the naive kernel updates in place)
   float scale[6] = {1, 1, 1, 1, 1, 1}, inv_scale[6] = {1, 1, 1, 1, 1, 1};
   float* f32_stage = nullptr;   // pitched FP32 staging for field transfers of other storages
@@ -103,6 +103,17 @@ struct fdtd_handle {
 };
 
 namespace {
+
+// Storage format of component c (0..5 = Ex Ey Ez Hx Hy Hz): F16E keeps E in FP16 and H in FP32.
+int comp_storage(const fdtd_handle* h, int c) {
+  if (h->storage == FDTD_STORE_F16E) return c < 3 ? FDTD_STORE_F16 : FDTD_STORE_F32;
+  return h->storage;
+}
+
+int comp_esz(const fdtd_handle* h, int c) {
+  const int s = comp_storage(h, c);
+  return s == FDTD_STORE_F32 ? 4 : (s == FDTD_STORE_F64 ? 8 : 2);
+}
 
 fdtd_status fail(fdtd_handle* h, fdtd_status s, const char* fmt, ...) {
   char buf[512];
@@ -162,12 +173,13 @@ fdtd_status encode_map(fdtd_handle* h, CUtensorMap* m, void* base, CUtensorMapDa
 fdtd_status ensure_maps(fdtd_handle* h, int width, int rows) {
   const int key = width * 1000 + rows;
   if (h->maps_key == key) return FDTD_OK;
-  const CUtensorMapDataType dt = h->storage == FDTD_STORE_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
-                                 : h->storage == FDTD_STORE_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                                                 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   for (int s = 0; s < 2; ++s)
     for (int c = 0; c < 6; ++c) {
-      fdtd_status st = encode_map(h, &h->maps[s][c], h->F[s][c], dt, h->esz, width, rows);
+      const int cs = comp_storage(h, c);
+      const CUtensorMapDataType dt = cs == FDTD_STORE_F16    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                     : cs == FDTD_STORE_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                             : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+      fdtd_status st = encode_map(h, &h->maps[s][c], h->F[s][c], dt, comp_esz(h, c), width, rows);
       if (st != FDTD_OK) return st;
     }
   const int mat_box = width == 64 ? fdtd::kMatBoxX2 : fdtd::kMatBoxX;
@@ -305,7 +317,7 @@ std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
 // and monitors off, so the simulation state is not changed) and keeps the fastest per step.
 fdtd_status autotune(fdtd_handle* h, cudaStream_t st) {
   const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz,
-                                   h->storage * 1000000000 + h->desc.min_blocks * 100000000 +
+                                   h->storage * 1000000000LL + h->desc.min_blocks * 100000000LL +
                                        h->desc.kernel * 1000000 + h->desc.blt * 10000 +
                                        h->desc.tile_rows * 100 + h->desc.z_chunks);
   {
@@ -502,11 +514,12 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "grid must be at least 3 cells per axis");
   if (d->nx > (1 << 24) || d->ny > (1 << 24) || d->nz > (1 << 24))
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "grid axis too large");
-  if (d->storage < FDTD_STORE_F32 || d->storage > FDTD_STORE_F64)
+  if (d->storage < FDTD_STORE_F32 || d->storage > FDTD_STORE_F16E)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "unknown storage %d", d->storage);
   if (d->kernel < FDTD_KERNEL_AUTO || d->kernel > FDTD_KERNEL_TILED_W32P)
     return fail(nullptr, FDTD_ERR_INVALID_ARG, "unknown kernel %d", d->kernel);
-  if ((d->storage == FDTD_STORE_F16 || d->storage == FDTD_STORE_BF16) &&
+  if ((d->storage == FDTD_STORE_F16 || d->storage == FDTD_STORE_BF16 ||
+       d->storage == FDTD_STORE_F16E) &&
       (d->kernel == FDTD_KERNEL_NAIVE || d->kernel == FDTD_KERNEL_TILED_W32))
     return fail(nullptr, FDTD_ERR_UNSUPPORTED,
                 "16-bit field storage runs the tiled x-pair kernel only");
@@ -547,11 +560,12 @@ fdtd_status fdtd_create(const fdtd_desc* d, fdtd_handle** out) {
     return bail(fail(h, FDTD_ERR_CUDA, "cudaStreamCreate failed"));
   for (int s = 0; s < h->nsets; ++s)
     for (int c = 0; c < 6; ++c) {
-      cudaError_t e = cudaMalloc(&h->F[s][c], h->cells * h->esz);
+      const size_t bytes = h->cells * (size_t)comp_esz(h, c);
+      cudaError_t e = cudaMalloc(&h->F[s][c], bytes);
       if (e != cudaSuccess)
-        return bail(fail(h, FDTD_ERR_OOM, "cudaMalloc of %zu field bytes failed: %s",
-                         h->cells * (size_t)h->esz, cudaGetErrorString(e)));
-      cudaMemsetAsync(h->F[s][c], 0, h->cells * h->esz, h->stream);
+        return bail(fail(h, FDTD_ERR_OOM, "cudaMalloc of %zu field bytes failed: %s", bytes,
+                         cudaGetErrorString(e)));
+      cudaMemsetAsync(h->F[s][c], 0, bytes, h->stream);
     }
   if (cudaMalloc(&h->d_err, sizeof(int)) != cudaSuccess)
     return bail(fail(h, FDTD_ERR_OOM, "cudaMalloc failed"));
@@ -714,7 +728,7 @@ fdtd_status fdtd_reset(fdtd_handle* h) {
   DeviceGuard dg(h->desc.device);
   for (int s = 0; s < h->nsets; ++s)
     for (int c = 0; c < 6; ++c)
-      CUDA_TRY(h, cudaMemsetAsync(h->F[s][c], 0, h->cells * h->esz, h->stream));
+      CUDA_TRY(h, cudaMemsetAsync(h->F[s][c], 0, h->cells * comp_esz(h, c), h->stream));
   for (int m = 0; m < h->nmon; ++m) {
     const size_t bytes = (size_t)h->mon[m].nf * h->g.nx * h->g.ny * sizeof(double);
     CUDA_TRY(h, cudaMemsetAsync(h->mon[m].re, 0, bytes, h->stream));
@@ -839,12 +853,12 @@ fdtd_status fdtd_get_step(const fdtd_handle* h, int64_t* t) {
 // Pitched FP32 view of a field component: the field itself for FP32 storage, else the
 // component converted into the FP32 staging buffer (asynchronous on st).
 fdtd_status f32_view(fdtd_handle* h, int32_t component, cudaStream_t st, const float** out) {
-  if (h->storage == FDTD_STORE_F32) {
+  if (comp_storage(h, component) == FDTD_STORE_F32) {
     *out = h->F[h->cur][component];
     return FDTD_OK;
   }
   if (!h->f32_stage) CUDA_TRY(h, cudaMalloc(&h->f32_stage, h->cells * sizeof(float)));
-  CUDA_TRY(h, fdtd::convert_field_to_f32(h->g, h->F[h->cur][component], h->storage,
+  CUDA_TRY(h, fdtd::convert_field_to_f32(h->g, h->F[h->cur][component], comp_storage(h, component),
                                          h->scale[component], h->f32_stage, st));
   *out = h->f32_stage;
   return FDTD_OK;
@@ -867,8 +881,9 @@ fdtd_status fdtd_get_field_f64(fdtd_handle* h, int32_t component, double* host_o
   if (!h || !host_out || component < 0 || component > 5) return FDTD_ERR_INVALID_ARG;
   DeviceGuard dg(h->desc.device);
   if (!h->f64_stage) CUDA_TRY(h, cudaMalloc(&h->f64_stage, h->cells * sizeof(double)));
-  CUDA_TRY(h, fdtd::convert_field_to_f64(h->g, h->F[h->cur][component], h->storage,
-                                         h->scale[component], h->f64_stage, h->stream));
+  CUDA_TRY(h, fdtd::convert_field_to_f64(h->g, h->F[h->cur][component],
+                                         comp_storage(h, component), h->scale[component],
+                                         h->f64_stage, h->stream));
   CUDA_TRY(h, cudaMemcpy2DAsync(host_out, (size_t)h->g.nx * 8, h->f64_stage,
                                 (size_t)h->g.pitch * 8, (size_t)h->g.nx * 8,
                                 (size_t)h->g.ny * h->g.nz, cudaMemcpyDeviceToHost, h->stream));
@@ -893,7 +908,7 @@ fdtd_status fdtd_get_field_device(fdtd_handle* h, int32_t component, float* dev_
 fdtd_status fdtd_set_field(fdtd_handle* h, int32_t component, const float* host_in) {
   if (!h || !host_in || component < 0 || component > 5) return FDTD_ERR_INVALID_ARG;
   DeviceGuard dg(h->desc.device);
-  if (h->storage == FDTD_STORE_F32) {
+  if (comp_storage(h, component) == FDTD_STORE_F32) {
     CUDA_TRY(h, cudaMemcpy2DAsync(h->F[h->cur][component], (size_t)h->g.pitch * 4, host_in,
                                   (size_t)h->g.nx * 4, (size_t)h->g.nx * 4,
                                   (size_t)h->g.ny * h->g.nz, cudaMemcpyHostToDevice, h->stream));
@@ -905,7 +920,7 @@ fdtd_status fdtd_set_field(fdtd_handle* h, int32_t component, const float* host_
     CUDA_TRY(h, cudaMemcpy2DAsync(h->f32_stage, (size_t)h->g.pitch * 4, host_in,
                                   (size_t)h->g.nx * 4, (size_t)h->g.nx * 4,
                                   (size_t)h->g.ny * h->g.nz, cudaMemcpyHostToDevice, h->stream));
-    CUDA_TRY(h, fdtd::convert_field_from_f32(h->g, h->f32_stage, h->storage,
+    CUDA_TRY(h, fdtd::convert_field_from_f32(h->g, h->f32_stage, comp_storage(h, component),
                                              h->inv_scale[component], h->F[h->cur][component],
                                              h->stream));
   }
@@ -945,7 +960,7 @@ fdtd_status plane_copy(fdtd_handle* h, int32_t comp, int64_t k0, int64_t nk, voi
     return FDTD_ERR_INVALID_ARG;
   DeviceGuard dg(h->desc.device);
   cudaStream_t st = pick_stream(h, stream);
-  const size_t esz = (size_t)h->esz;
+  const size_t esz = (size_t)comp_esz(h, comp);
   char* field = reinterpret_cast<char*>(h->F[h->cur][comp]) + (size_t)k0 * h->g.plane * esz;
   char* packed = static_cast<char*>(dev);
   const size_t row = (size_t)h->g.nx * esz, pitch = (size_t)h->g.pitch * esz;
@@ -973,13 +988,19 @@ fdtd_status fdtd_storage_bytes(const fdtd_handle* h, int32_t* esz) {
   return FDTD_OK;
 }
 
+fdtd_status fdtd_component_bytes(const fdtd_handle* h, int32_t component, int32_t* esz) {
+  if (!h || !esz || component < 0 || component > 5) return FDTD_ERR_INVALID_ARG;
+  *esz = comp_esz(h, component);
+  return FDTD_OK;
+}
+
 fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6) {
   if (!h || !scale6) return FDTD_ERR_INVALID_ARG;
   for (int c = 0; c < 6; ++c)
     if (!(scale6[c] > 0.0f) || !std::isfinite(scale6[c]))
       return fail(h, FDTD_ERR_INVALID_ARG, "storage scale %d must be positive and finite", c);
-  if (h->esz != 2) return FDTD_OK;  // FP32 / FP64 storage is unscaled
   for (int c = 0; c < 6; ++c) {
+    if (comp_esz(h, c) != 2) continue;  // FP32 / FP64 components are unscaled
     const int e = (int)std::lround(std::log2((double)scale6[c]));
     if (e < -100 || e > 100) return fail(h, FDTD_ERR_INVALID_ARG, "storage scale out of range");
     h->scale[c] = std::ldexp(1.0f, e);

@@ -61,8 +61,8 @@ struct TiledConfig {
   int z_chunks;   // z-chunks per tile column
   int width = 32; // cells per warp row: 32 (k_tiled.cu) or 64 (k_tiled2.cu, x-pairs)
   int min_blocks = 1;  // register cap: CTAs per SM the compiler must fit (x-pair family)
-  int storage = 0;     // 0 FP32, 1 FP16, 2 BF16 (x-pair family only for 16-bit)
-  int esz = 4;         // bytes per stored field value
+  int storage = 0;     // 0 FP32, 1 FP16, 2 BF16, 4 FP16 E + FP32 H (x-pair family for all but 0)
+  int esz = 4;         // bytes per stored field value (the narrower of E and H)
   bool pairs32 = false;  // x-pair kernel with 32-cell rows, two per warp (width must be 32)
 };
 

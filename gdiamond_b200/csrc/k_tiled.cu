@@ -330,7 +330,7 @@ size_t smem_of() { return Tiled<B, TY>::SMEM; }
 }  // namespace
 
 bool tiled_config_supported(const TiledConfig& c) {
-  if (c.min_blocks != 1 || c.pairs32) return false;
+  if (c.min_blocks != 1 || c.pairs32 || c.storage != 0) return false;  // FP32 fields only
   if (c.rows != 8 && c.rows != 16 && c.rows != 32) return false;
   if (c.blt < 1 || c.blt > 6) return false;
   if (c.rows == 8 && c.blt > 3) return false;

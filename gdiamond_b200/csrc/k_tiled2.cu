@@ -12,15 +12,16 @@
 //  * the x-trapezoid wastes 2*BLT of 64 columns instead of 2*BLT of 32;
 //  * source and monitor planes are tested once per z-iteration against CTA-uniform ranges.
 //
-// Field storage S is float, __half or __nv_bfloat16.  Arithmetic is FP32 in every case and the
+// Field storage S is float, __half or __nv_bfloat16 for E, and SH (default S) for H: <__half,
+// float> keeps E in FP16 and H in FP32.  Arithmetic is FP32 in every case and the
 // intermediate time levels never leave the SM in reduced precision: only the HBM round trip of
 // each BLT-step pass is 16-bit.  A 16-bit value v is stored as v * inv_scale[c] and read back
 // times scale[c]; scales are powers of two, so the scaling itself rounds nothing.  With FP32
 // storage no scaling is applied and every multiply/add is separately rounded: results are
 // bit-identical to the reference CPU update.
 //
-// x tile starts are multiples of 16 bytes of the stored type (4 floats, 8 halves): the TMA rule
-// for the innermost coordinate.
+// x tile starts are multiples of 16 bytes of the narrower stored type (4 floats, 8 halves): the
+// TMA rule for the innermost coordinate, for both types.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -80,20 +81,23 @@ struct Store<__nv_bfloat16> {
 // W = 64: one 64-cell row per warp (32 lanes x an x-pair).  W = 32: two 32-cell rows per warp
 // (16 lanes x an x-pair each), so a CTA of the same 16 warps covers a 32 x 32 tile instead of
 // 64 x 16: more of it valid under the trapezoid and a finer x granularity on small grids.
-template <typename S, int B, int TY, int W = 64>
+template <typename S, int B, int TY, int W = 64, typename SH = S>
 struct Tiled2 {
-  static constexpr int ESZ = (int)sizeof(S);
+  static constexpr int ESZ_E = (int)sizeof(S);    // stored E value
+  static constexpr int ESZ_H = (int)sizeof(SH);   // stored H value
+  static constexpr int ESZ = ESZ_E < ESZ_H ? ESZ_E : ESZ_H;  // x alignment unit
   static constexpr int LPR = W / 2;            // lanes per tile row
   static constexpr int THREADS = TY * LPR;
   static constexpr int MBX = W == 64 ? kMatBoxX2 : kMatBoxX;  // material box width
   static constexpr int PL = W * TY;            // elements of one staged field plane
   static constexpr int MPL = MBX * TY;         // elements of one staged material plane
   static constexpr int MPL_S = (MPL * 2 + 127) / 128 * 64;  // its stage stride: 128-byte steps
-  static constexpr int NS = ESZ == 4 ? kTiled2Stages : kTiled2Stages + 1;
+  static constexpr int NS = ESZ_E + ESZ_H == 8 ? kTiled2Stages : kTiled2Stages + 1;
   static constexpr int SX = tiled2_sx_w(W, B, ESZ);
   static constexpr int SY = tiled_sy(B, TY);
   static constexpr int XBASE = tiled2_xbase(B, ESZ);
-  static constexpr uint32_t STAGE_F_BYTES = 6u * PL * ESZ;
+  static constexpr uint32_t OFF_HPLANES = 3u * PL * ESZ_E;  // H planes follow E in a stage
+  static constexpr uint32_t STAGE_F_BYTES = 3u * PL * (ESZ_E + ESZ_H);
   static constexpr uint32_t STAGE_M_BYTES = MPL_S * 2u;  // TMA destinations stay 128-aligned
   static constexpr uint32_t TX_BYTES = STAGE_F_BYTES + MPL * 2u;  // bytes the copies deliver
   static constexpr size_t OFF_M = (size_t)NS * STAGE_F_BYTES;
@@ -104,6 +108,7 @@ struct Tiled2 {
   static_assert(SY >= 1, "tile too short for this BLT");
   static_assert((W == 64 || W == 32) && THREADS % 32 == 0, "warp rows of 64 or 32 cells");
   static_assert(STAGE_M_BYTES % 128 == 0 && (PL * ESZ) % 128 == 0, "stage alignment");
+  static_assert(STAGE_F_BYTES % 128 == 0, "stage alignment");
 };
 
 struct Pair {
@@ -128,12 +133,13 @@ struct Smem {
 // `gbase` counts the pipeline stages this CTA consumed before (mbarrier phases continue across
 // tiles in the persistent form).  Every thread of the CTA calls it; returns false when a
 // bounded wait expired (the CTA must then stop).
-template <typename S, int B, int TY, int W = 64>
+template <typename S, int B, int TY, int W = 64, typename SH = S>
 __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz,
                                       const Smem& sm, uint32_t& gbase, long long t_offset) {
-  using K = Tiled2<S, B, TY, W>;
-  using St = Store<S>;
-  S* st_f = reinterpret_cast<S*>(sm.base);
+  using K = Tiled2<S, B, TY, W, SH>;
+  using St = Store<S>;    // E components
+  using StH = Store<SH>;  // H components
+  unsigned char* st_f = sm.base;  // per stage: Ex Ey Ez as S, then Hx Hy Hz as SH
   uint16_t* st_m = reinterpret_cast<uint16_t*>(sm.base + K::OFF_M);
   float* hbuf = reinterpret_cast<float*>(sm.base + K::OFF_H);  // [2][Hz,Hx][PL]
   float* ebuf = reinterpret_cast<float*>(sm.base + K::OFF_E);  // [B][Ex,Ez][PL]
@@ -149,7 +155,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   const int lx = threadIdx.x % K::LPR;                                   // pair in the row
   const int ly = threadIdx.y * (32 / K::LPR) + threadIdx.x / K::LPR;     // tile row
   const int tid = threadIdx.y * 32 + threadIdx.x;
-  const int X = bx * K::SX + K::XBASE;  // multiple of 16 bytes of S
+  const int X = bx * K::SX + K::XBASE;  // multiple of 16 bytes of S and of SH
   const int Y = by * K::SY - B;
   const int X8 = X & ~7;
   const int cx0 = 2 * lx;               // tile column of the even cell
@@ -184,8 +190,9 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   float sc[6], inv[6];
 #pragma unroll
   for (int c = 0; c < 6; ++c) {
-    sc[c] = St::kScaled ? a.scale[c] : 1.0f;
-    inv[c] = St::kScaled ? a.inv_scale[c] : 1.0f;
+    const bool scaled = c < 3 ? St::kScaled : StH::kScaled;
+    sc[c] = scaled ? a.scale[c] : 1.0f;
+    inv[c] = scaled ? a.inv_scale[c] : 1.0f;
   }
 
   for (int q = tid; q < (4 + 2 * B) * K::PL; q += K::THREADS) hbuf[q] = 0.0f;
@@ -196,10 +203,15 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     const int stage = (int)(u % K::NS);
     uint64_t* bar = &bars[stage];
     mbar_arrive_expect_tx(bar, K::TX_BYTES);
-    S* d = st_f + stage * 6 * K::PL;
+    unsigned char* d = st_f + stage * K::STAGE_F_BYTES;
+    S* de = reinterpret_cast<S*>(d);
+    SH* dh = reinterpret_cast<SH*>(d + K::OFF_HPLANES);
     const int pz = ps + it_;
 #pragma unroll
-    for (int c = 0; c < 6; ++c) tma_load_3d(d + c * K::PL, &a.tm_src[c], bar, X, Y, pz);
+    for (int c = 0; c < 3; ++c) {
+      tma_load_3d(de + c * K::PL, &a.tm_src[c], bar, X, Y, pz);
+      tma_load_3d(dh + c * K::PL, &a.tm_src[3 + c], bar, X, Y, pz);
+    }
     tma_load_3d(st_m + stage * K::MPL_S, &a.tm_mat, bar, X8, Y, pz);
   };
   if (tid == 0) {
@@ -223,7 +235,8 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   const int om = ly * K::MBX + cx0 + (X - X8);  // even: a 4-byte aligned id pair
   const float dx = a.dx;
   const long long pitch = g.pitch, plane = g.plane;
-  S* const* dst = reinterpret_cast<S* const*>(a.dst.f);
+  S* const* dst = reinterpret_cast<S* const*>(a.dst.f);        // E components
+  SH* const* dsth = reinterpret_cast<SH* const*>(a.dst.f + 3);  // H components
 
   int it = 0;
   bool abort = false;
@@ -239,20 +252,21 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     const bool mon_iter = p >= mon_lo && p <= mon_hi;
     const bool src_iter = smask != 0 && p >= src_lo && p <= src_hi;
 
-    const S* S0 = st_f + stage * 6 * K::PL;
+    const S* E0 = reinterpret_cast<const S*>(st_f + stage * K::STAGE_F_BYTES);
+    const SH* H0 = reinterpret_cast<const SH*>(st_f + stage * K::STAGE_F_BYTES + K::OFF_HPLANES);
 #pragma unroll
     for (int s = B; s >= 1; --s) mq[s] = mq[s - 1];
     mq[0] = *reinterpret_cast<const uint32_t*>(st_m + stage * K::MPL_S + om);
     Pair Hc[3], Eo[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float2 hv = St::ld2(S0 + (3 + c) * K::PL + o, sc[3 + c]);
-      const float2 ev = St::ld2(S0 + c * K::PL + o, sc[c]);
+      const float2 hv = StH::ld2(H0 + c * K::PL + o, sc[3 + c]);
+      const float2 ev = St::ld2(E0 + c * K::PL + o, sc[c]);
       Hc[c] = Pair{hv.x, hv.y};
       Eo[c] = Pair{ev.x, ev.y};
     }
-    float2 hz_ym = St::ld2(S0 + 5 * K::PL + oym, sc[5]);
-    float2 hx_ym = St::ld2(S0 + 3 * K::PL + oym, sc[3]);
+    float2 hz_ym = StH::ld2(H0 + 2 * K::PL + oym, sc[5]);
+    float2 hx_ym = StH::ld2(H0 + oym, sc[3]);
     Pair EnPrev[3] = {};
     Pair EnB[3] = {}, HnB[3] = {};
 
@@ -414,9 +428,9 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
         const long long idx = x0 + (long long)y * pitch + (long long)hB * plane;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          if (both) St::st2(dst[3 + c] + idx, HnB[c].a, HnB[c].b, inv[3 + c]);
-          else if (out0) St::st1(dst[3 + c] + idx, HnB[c].a, inv[3 + c]);
-          else St::st1(dst[3 + c] + idx + 1, HnB[c].b, inv[3 + c]);
+          if (both) StH::st2(dsth[c] + idx, HnB[c].a, HnB[c].b, inv[3 + c]);
+          else if (out0) StH::st1(dsth[c] + idx, HnB[c].a, inv[3 + c]);
+          else StH::st1(dsth[c] + idx + 1, HnB[c].b, inv[3 + c]);
         }
       }
     }
@@ -436,9 +450,9 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   return true;
 }
 
-template <typename S, int B, int TY, int W = 64>
+template <typename S, int B, int TY, int W = 64, typename SH = S>
 __device__ __forceinline__ Smem setup_smem(unsigned char* smem_raw, int* s_abort) {
-  using K = Tiled2<S, B, TY, W>;
+  using K = Tiled2<S, B, TY, W, SH>;
   unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   Smem sm{base, reinterpret_cast<uint64_t*>(base + K::OFF_BAR), s_abort};
   if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -451,23 +465,24 @@ __device__ __forceinline__ Smem setup_smem(unsigned char* smem_raw, int* s_abort
 
 // One grid: one tile per CTA.  MINB > 1 caps registers so that MINB CTAs fit on an SM (more
 // warps to hide latency, at the cost of some spilled state); the autotuner decides.
-template <typename S, int B, int TY, int MINB, int W = 64>
+template <typename S, int B, int TY, int MINB, int W = 64, typename SH = S>
 __global__ void __launch_bounds__(TY * W / 2, MINB)
     fdtd_tiled2(const __grid_constant__ TiledArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_abort;
-  const Smem sm = setup_smem<S, B, TY, W>(smem_raw, &s_abort);
+  const Smem sm = setup_smem<S, B, TY, W, SH>(smem_raw, &s_abort);
   uint32_t gbase = 0;
-  (void)march<S, B, TY, W>(a, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, sm, gbase, 0);
+  (void)march<S, B, TY, W, SH>(a, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, sm, gbase,
+                               0);
 }
 
 // A batch of independent grids: persistent CTAs pull (grid, tile) work items from a queue.
-template <typename S, int B, int TY, int W = 64>
+template <typename S, int B, int TY, int W = 64, typename SH = S>
 __global__ void __launch_bounds__(TY * W / 2, 1) fdtd_tiled2_batch(const BatchArgs b) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_abort;
   __shared__ int s_item;
-  const Smem sm = setup_smem<S, B, TY, W>(smem_raw, &s_abort);
+  const Smem sm = setup_smem<S, B, TY, W, SH>(smem_raw, &s_abort);
   const int tid = threadIdx.y * 32 + threadIdx.x;
   uint32_t gbase = 0;
   while (true) {
@@ -478,131 +493,134 @@ __global__ void __launch_bounds__(TY * W / 2, 1) fdtd_tiled2_batch(const BatchAr
     if (item >= b.nitems) break;
     const int4 w = b.items[item];  // {grid, bx, by, bz}
     const TiledArgs& a = b.grids[b.flip * b.ngrids + w.x];
-    if (!march<S, B, TY, W>(a, w.y, w.z, w.w, sm, gbase, b.t_offset)) break;
+    if (!march<S, B, TY, W, SH>(a, w.y, w.z, w.w, sm, gbase, b.t_offset)) break;
   }
 }
 
-template <typename S, int B, int TY, int MINB, int W = 64>
+template <typename S, int B, int TY, int MINB, int W = 64, typename SH = S>
 cudaError_t launch_one2(const TiledArgs& a, dim3 grid, cudaStream_t st) {
-  using K = Tiled2<S, B, TY, W>;
-  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2<S, B, TY, MINB, W>,
+  using K = Tiled2<S, B, TY, W, SH>;
+  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2<S, B, TY, MINB, W, SH>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
   if (e != cudaSuccess) return e;
-  fdtd_tiled2<S, B, TY, MINB, W><<<grid, dim3(32, K::THREADS / 32), K::SMEM, st>>>(a);
+  fdtd_tiled2<S, B, TY, MINB, W, SH><<<grid, dim3(32, K::THREADS / 32), K::SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
-template <typename S, int B, int TY, int W = 64>
+template <typename S, int B, int TY, int W = 64, typename SH = S>
 cudaError_t launch_batch_one(const BatchArgs& b, int ctas, cudaStream_t st) {
-  using K = Tiled2<S, B, TY, W>;
-  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2_batch<S, B, TY, W>,
+  using K = Tiled2<S, B, TY, W, SH>;
+  cudaError_t e = cudaFuncSetAttribute(fdtd_tiled2_batch<S, B, TY, W, SH>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
   if (e != cudaSuccess) return e;
-  fdtd_tiled2_batch<S, B, TY, W><<<ctas, dim3(32, K::THREADS / 32), K::SMEM, st>>>(b);
+  fdtd_tiled2_batch<S, B, TY, W, SH><<<ctas, dim3(32, K::THREADS / 32), K::SMEM, st>>>(b);
   return cudaGetLastError();
 }
 
 // 32-wide rows (two per warp): 32 rows (16 warps, BLT 1-3) or 48 rows (24 warps, BLT 1-2).
-template <typename S>
+template <typename S, typename SH = S>
 cudaError_t launch_pairs32(int blt, int rows, const TiledArgs& a, dim3 grid, cudaStream_t st) {
   if (rows == 32) {
     switch (blt) {
-      case 1: return launch_one2<S, 1, 32, 1, 32>(a, grid, st);
-      case 2: return launch_one2<S, 2, 32, 1, 32>(a, grid, st);
-      case 3: return launch_one2<S, 3, 32, 1, 32>(a, grid, st);
+      case 1: return launch_one2<S, 1, 32, 1, 32, SH>(a, grid, st);
+      case 2: return launch_one2<S, 2, 32, 1, 32, SH>(a, grid, st);
+      case 3: return launch_one2<S, 3, 32, 1, 32, SH>(a, grid, st);
       default: break;
     }
   } else if (rows == 48) {
     switch (blt) {
-      case 1: return launch_one2<S, 1, 48, 1, 32>(a, grid, st);
-      case 2: return launch_one2<S, 2, 48, 1, 32>(a, grid, st);
+      case 1: return launch_one2<S, 1, 48, 1, 32, SH>(a, grid, st);
+      case 2: return launch_one2<S, 2, 48, 1, 32, SH>(a, grid, st);
       default: break;
     }
   }
   return cudaErrorInvalidValue;
 }
 
-template <typename S>
+template <typename S, typename SH = S>
 cudaError_t launch_batch_pairs32(int blt, int rows, const BatchArgs& b, int ctas,
                                  cudaStream_t st) {
   if (rows == 32) {
     switch (blt) {
-      case 1: return launch_batch_one<S, 1, 32, 32>(b, ctas, st);
-      case 2: return launch_batch_one<S, 2, 32, 32>(b, ctas, st);
-      case 3: return launch_batch_one<S, 3, 32, 32>(b, ctas, st);
+      case 1: return launch_batch_one<S, 1, 32, 32, SH>(b, ctas, st);
+      case 2: return launch_batch_one<S, 2, 32, 32, SH>(b, ctas, st);
+      case 3: return launch_batch_one<S, 3, 32, 32, SH>(b, ctas, st);
       default: break;
     }
   } else if (rows == 48) {
     switch (blt) {
-      case 1: return launch_batch_one<S, 1, 48, 32>(b, ctas, st);
-      case 2: return launch_batch_one<S, 2, 48, 32>(b, ctas, st);
+      case 1: return launch_batch_one<S, 1, 48, 32, SH>(b, ctas, st);
+      case 2: return launch_batch_one<S, 2, 48, 32, SH>(b, ctas, st);
       default: break;
     }
   }
   return cudaErrorInvalidValue;
 }
 
-template <typename S, int TY>
+template <typename S, int TY, typename SH = S>
 cudaError_t launch_rows2(int blt, int min_blocks, const TiledArgs& a, dim3 grid,
                          cudaStream_t st) {
   if (min_blocks > 1) {
     // register-capped FP32 variants: two CTAs of 16 rows or four of 8 rows per SM
-    if constexpr (sizeof(S) == 4 && TY == 16) {
+    if constexpr (sizeof(S) == 4 && sizeof(SH) == 4 && TY == 16) {
       if (blt == 2 && min_blocks == 2) return launch_one2<S, 2, 16, 2>(a, grid, st);
     }
-    if constexpr (sizeof(S) == 4 && TY == 8) {
+    if constexpr (sizeof(S) == 4 && sizeof(SH) == 4 && TY == 8) {
       if (blt == 2 && min_blocks == 4) return launch_one2<S, 2, 8, 4>(a, grid, st);
     }
     return cudaErrorInvalidValue;
   }
   switch (blt) {
-    case 1: return launch_one2<S, 1, TY, 1>(a, grid, st);
-    case 2: return launch_one2<S, 2, TY, 1>(a, grid, st);
-    case 3: if constexpr (TY <= 20) return launch_one2<S, 3, TY, 1>(a, grid, st); break;
-    case 4: if constexpr (TY == 16) return launch_one2<S, 4, TY, 1>(a, grid, st); break;
+    case 1: return launch_one2<S, 1, TY, 1, 64, SH>(a, grid, st);
+    case 2: return launch_one2<S, 2, TY, 1, 64, SH>(a, grid, st);
+    case 3: if constexpr (TY <= 20) return launch_one2<S, 3, TY, 1, 64, SH>(a, grid, st); break;
+    case 4: if constexpr (TY == 16) return launch_one2<S, 4, TY, 1, 64, SH>(a, grid, st); break;
     default: break;
   }
   return cudaErrorInvalidValue;
 }
 
-template <typename S>
+template <typename S, typename SH = S>
 cudaError_t launch_type2(const TiledConfig& c, const TiledArgs& a, dim3 grid, cudaStream_t st) {
   switch (c.rows) {
-    case 8: return launch_rows2<S, 8>(c.blt, c.min_blocks, a, grid, st);
-    case 16: return launch_rows2<S, 16>(c.blt, c.min_blocks, a, grid, st);
+    case 8: return launch_rows2<S, 8, SH>(c.blt, c.min_blocks, a, grid, st);
+    case 16: return launch_rows2<S, 16, SH>(c.blt, c.min_blocks, a, grid, st);
     case 20:  // FP32: 640 threads, the register file's limit at ~96 registers per thread
-      if constexpr (sizeof(S) == 4) return launch_rows2<S, 20>(c.blt, c.min_blocks, a, grid, st);
+      if constexpr (sizeof(S) == 4 && sizeof(SH) == 4)
+        return launch_rows2<S, 20>(c.blt, c.min_blocks, a, grid, st);
       break;
     case 24:
-      if constexpr (sizeof(S) == 4) return launch_rows2<S, 24>(c.blt, c.min_blocks, a, grid, st);
+      if constexpr (sizeof(S) == 4 && sizeof(SH) == 4)
+        return launch_rows2<S, 24>(c.blt, c.min_blocks, a, grid, st);
       break;
     case 32:
-      if constexpr (sizeof(S) == 4) return launch_rows2<S, 32>(c.blt, c.min_blocks, a, grid, st);
+      if constexpr (sizeof(S) == 4 && sizeof(SH) == 4)
+        return launch_rows2<S, 32>(c.blt, c.min_blocks, a, grid, st);
       break;
     default: break;
   }
   return cudaErrorInvalidValue;
 }
 
-template <typename S>
+template <typename S, typename SH = S>
 cudaError_t launch_batch_type(const TiledConfig& c, const BatchArgs& b, int ctas,
                               cudaStream_t st) {
   if (c.rows == 16) {
     switch (c.blt) {
-      case 1: return launch_batch_one<S, 1, 16>(b, ctas, st);
-      case 2: return launch_batch_one<S, 2, 16>(b, ctas, st);
-      case 3: return launch_batch_one<S, 3, 16>(b, ctas, st);
-      case 4: return launch_batch_one<S, 4, 16>(b, ctas, st);
+      case 1: return launch_batch_one<S, 1, 16, 64, SH>(b, ctas, st);
+      case 2: return launch_batch_one<S, 2, 16, 64, SH>(b, ctas, st);
+      case 3: return launch_batch_one<S, 3, 16, 64, SH>(b, ctas, st);
+      case 4: return launch_batch_one<S, 4, 16, 64, SH>(b, ctas, st);
       default: break;
     }
   } else if (c.rows == 8) {
     switch (c.blt) {
-      case 1: return launch_batch_one<S, 1, 8>(b, ctas, st);
-      case 2: return launch_batch_one<S, 2, 8>(b, ctas, st);
-      case 3: return launch_batch_one<S, 3, 8>(b, ctas, st);
+      case 1: return launch_batch_one<S, 1, 8, 64, SH>(b, ctas, st);
+      case 2: return launch_batch_one<S, 2, 8, 64, SH>(b, ctas, st);
+      case 3: return launch_batch_one<S, 3, 8, 64, SH>(b, ctas, st);
       default: break;
     }
-  } else if constexpr (sizeof(S) == 4) {
+  } else if constexpr (sizeof(S) == 4 && sizeof(SH) == 4) {
     if (c.rows == 20) {
       switch (c.blt) {
         case 1: return launch_batch_one<S, 1, 20>(b, ctas, st);
@@ -621,19 +639,19 @@ cudaError_t launch_batch_type(const TiledConfig& c, const BatchArgs& b, int ctas
   return cudaErrorInvalidValue;
 }
 
-template <typename S, int B, int TY, int W = 64>
+template <typename S, int B, int TY, int W = 64, typename SH = S>
 size_t smem_of() {
-  return Tiled2<S, B, TY, W>::SMEM;
+  return Tiled2<S, B, TY, W, SH>::SMEM;
 }
 
-template <typename S, int B, int TY, int W = 64>
+template <typename S, int B, int TY, int W = 64, typename SH = S>
 int occupancy_of() {
-  using K = Tiled2<S, B, TY, W>;
+  using K = Tiled2<S, B, TY, W, SH>;
   int n = 0;
-  cudaFuncSetAttribute(fdtd_tiled2_batch<S, B, TY, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)K::SMEM);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fdtd_tiled2_batch<S, B, TY, W>, K::THREADS,
-                                                    K::SMEM) != cudaSuccess)
+  cudaFuncSetAttribute(fdtd_tiled2_batch<S, B, TY, W, SH>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fdtd_tiled2_batch<S, B, TY, W, SH>,
+                                                    K::THREADS, K::SMEM) != cudaSuccess)
     return 1;
   return n > 0 ? n : 1;
 }
@@ -643,70 +661,53 @@ bool pairs32_supported(const TiledConfig& c) {
          ((c.rows == 32 && c.blt >= 1 && c.blt <= 3) || (c.rows == 48 && c.blt >= 1 && c.blt <= 2));
 }
 
-template <typename S>
-size_t pairs32_smem(const TiledConfig& c) {
-  if (c.rows == 32) {
-    switch (c.blt) {
-      case 1: return smem_of<S, 1, 32, 32>();
-      case 2: return smem_of<S, 2, 32, 32>();
-      case 3: return smem_of<S, 3, 32, 32>();
+// Shared memory (SMEM) or resident batch CTAs per SM (OCC) of the batch instance for config c.
+template <typename S, typename SH, bool OCC>
+size_t batch_query(const TiledConfig& c) {
+#define GD_Q(B, TY, W) (OCC ? (size_t)occupancy_of<S, B, TY, W, SH>() : smem_of<S, B, TY, W, SH>())
+  constexpr bool f32 = sizeof(S) == 4 && sizeof(SH) == 4;
+  if (c.pairs32) {
+    if (c.rows == 32) {
+      switch (c.blt) {
+        case 1: return GD_Q(1, 32, 32);
+        case 2: return GD_Q(2, 32, 32);
+        case 3: return GD_Q(3, 32, 32);
+      }
+    } else if (c.rows == 48) {
+      switch (c.blt) {
+        case 1: return GD_Q(1, 48, 32);
+        case 2: return GD_Q(2, 48, 32);
+      }
     }
-  } else if (c.rows == 48) {
+  } else if (c.rows == 16) {
     switch (c.blt) {
-      case 1: return smem_of<S, 1, 48, 32>();
-      case 2: return smem_of<S, 2, 48, 32>();
-    }
-  }
-  return 0;
-}
-
-template <typename S>
-int pairs32_occupancy(const TiledConfig& c) {
-  if (c.rows == 32) {
-    switch (c.blt) {
-      case 1: return occupancy_of<S, 1, 32, 32>();
-      case 2: return occupancy_of<S, 2, 32, 32>();
-      case 3: return occupancy_of<S, 3, 32, 32>();
-    }
-  } else if (c.rows == 48) {
-    switch (c.blt) {
-      case 1: return occupancy_of<S, 1, 48, 32>();
-      case 2: return occupancy_of<S, 2, 48, 32>();
-    }
-  }
-  return 1;
-}
-
-template <typename S>
-int batch_occupancy_type(const TiledConfig& c) {
-  if (c.rows == 16) {
-    switch (c.blt) {
-      case 1: return occupancy_of<S, 1, 16>();
-      case 2: return occupancy_of<S, 2, 16>();
-      case 3: return occupancy_of<S, 3, 16>();
-      case 4: return occupancy_of<S, 4, 16>();
+      case 1: return GD_Q(1, 16, 64);
+      case 2: return GD_Q(2, 16, 64);
+      case 3: return GD_Q(3, 16, 64);
+      case 4: return GD_Q(4, 16, 64);
     }
   } else if (c.rows == 8) {
     switch (c.blt) {
-      case 1: return occupancy_of<S, 1, 8>();
-      case 2: return occupancy_of<S, 2, 8>();
-      case 3: return occupancy_of<S, 3, 8>();
+      case 1: return GD_Q(1, 8, 64);
+      case 2: return GD_Q(2, 8, 64);
+      case 3: return GD_Q(3, 8, 64);
     }
-  } else if constexpr (sizeof(S) == 4) {
+  } else if constexpr (f32) {
     if (c.rows == 20) {
       switch (c.blt) {
-        case 1: return occupancy_of<S, 1, 20>();
-        case 2: return occupancy_of<S, 2, 20>();
-        case 3: return occupancy_of<S, 3, 20>();
+        case 1: return GD_Q(1, 20, 64);
+        case 2: return GD_Q(2, 20, 64);
+        case 3: return GD_Q(3, 20, 64);
       }
     } else if (c.rows == 24) {
       switch (c.blt) {
-        case 1: return occupancy_of<S, 1, 24>();
-        case 2: return occupancy_of<S, 2, 24>();
+        case 1: return GD_Q(1, 24, 64);
+        case 2: return GD_Q(2, 24, 64);
       }
     }
   }
-  return 1;
+#undef GD_Q
+  return OCC ? 1 : 0;
 }
 
 }  // namespace
@@ -747,60 +748,26 @@ dim3 tiled2_grid(const TiledConfig& c, const Grid& g) {
 }
 
 size_t tiled2_batch_smem(const TiledConfig& c) {
-  const bool h = c.esz == 2;
-  if (c.pairs32) {
-    switch (c.storage) {
-      case 0: return pairs32_smem<float>(c);
-      case 1: return pairs32_smem<__half>(c);
-      case 2: return pairs32_smem<__nv_bfloat16>(c);
-    }
-    return 0;
-  }
-  if (c.rows == 16) {
-    switch (c.blt) {
-      case 1: return h ? smem_of<__half, 1, 16>() : smem_of<float, 1, 16>();
-      case 2: return h ? smem_of<__half, 2, 16>() : smem_of<float, 2, 16>();
-      case 3: return h ? smem_of<__half, 3, 16>() : smem_of<float, 3, 16>();
-      case 4: return h ? smem_of<__half, 4, 16>() : smem_of<float, 4, 16>();
-    }
-  } else if (c.rows == 8) {
-    switch (c.blt) {
-      case 1: return h ? smem_of<__half, 1, 8>() : smem_of<float, 1, 8>();
-      case 2: return h ? smem_of<__half, 2, 8>() : smem_of<float, 2, 8>();
-      case 3: return h ? smem_of<__half, 3, 8>() : smem_of<float, 3, 8>();
-    }
-  } else if (c.rows == 20 && !h) {
-    switch (c.blt) {
-      case 1: return smem_of<float, 1, 20>();
-      case 2: return smem_of<float, 2, 20>();
-      case 3: return smem_of<float, 3, 20>();
-    }
-  } else if (c.rows == 24 && !h) {
-    switch (c.blt) {
-      case 1: return smem_of<float, 1, 24>();
-      case 2: return smem_of<float, 2, 24>();
-    }
+  switch (c.storage) {
+    case 0: return batch_query<float, float, false>(c);
+    case 1: return batch_query<__half, __half, false>(c);
+    case 2: return batch_query<__nv_bfloat16, __nv_bfloat16, false>(c);
+    case 4: return batch_query<__half, float, false>(c);
   }
   return 0;
 }
 
 int tiled2_batch_ctas_per_sm(const TiledConfig& c) {
-  if (c.pairs32) {
-    switch (c.storage) {
-      case 0: return pairs32_occupancy<float>(c);
-      case 1: return pairs32_occupancy<__half>(c);
-      case 2: return pairs32_occupancy<__nv_bfloat16>(c);
-    }
-    return 1;
-  }
   switch (c.storage) {
-    case 0: return batch_occupancy_type<float>(c);
-    case 1: return batch_occupancy_type<__half>(c);
-    case 2: return batch_occupancy_type<__nv_bfloat16>(c);
+    case 0: return (int)batch_query<float, float, true>(c);
+    case 1: return (int)batch_query<__half, __half, true>(c);
+    case 2: return (int)batch_query<__nv_bfloat16, __nv_bfloat16, true>(c);
+    case 4: return (int)batch_query<__half, float, true>(c);
   }
   return 1;
 }
 
+// storage: 0 FP32, 1 FP16, 2 BF16, 4 FP16 E with FP32 H.
 cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& a, const Grid& g,
                           cudaStream_t st) {
   if (!tiled2_config_supported(c)) return cudaErrorInvalidValue;
@@ -810,6 +777,7 @@ cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& a, const Grid& 
       case 0: return launch_pairs32<float>(c.blt, c.rows, a, grid, st);
       case 1: return launch_pairs32<__half>(c.blt, c.rows, a, grid, st);
       case 2: return launch_pairs32<__nv_bfloat16>(c.blt, c.rows, a, grid, st);
+      case 4: return launch_pairs32<__half, float>(c.blt, c.rows, a, grid, st);
       default: return cudaErrorInvalidValue;
     }
   }
@@ -817,6 +785,7 @@ cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& a, const Grid& 
     case 0: return launch_type2<float>(c, a, grid, st);
     case 1: return launch_type2<__half>(c, a, grid, st);
     case 2: return launch_type2<__nv_bfloat16>(c, a, grid, st);
+    case 4: return launch_type2<__half, float>(c, a, grid, st);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -829,6 +798,7 @@ cudaError_t launch_tiled2_batch(const TiledConfig& c, const BatchArgs& b, int ct
       case 0: return launch_batch_pairs32<float>(c.blt, c.rows, b, ctas, st);
       case 1: return launch_batch_pairs32<__half>(c.blt, c.rows, b, ctas, st);
       case 2: return launch_batch_pairs32<__nv_bfloat16>(c.blt, c.rows, b, ctas, st);
+      case 4: return launch_batch_pairs32<__half, float>(c.blt, c.rows, b, ctas, st);
       default: return cudaErrorInvalidValue;
     }
   }
@@ -836,6 +806,7 @@ cudaError_t launch_tiled2_batch(const TiledConfig& c, const BatchArgs& b, int ct
     case 0: return launch_batch_type<float>(c, b, ctas, st);
     case 1: return launch_batch_type<__half>(c, b, ctas, st);
     case 2: return launch_batch_type<__nv_bfloat16>(c, b, ctas, st);
+    case 4: return launch_batch_type<__half, float>(c, b, ctas, st);
     default: return cudaErrorInvalidValue;
   }
 }

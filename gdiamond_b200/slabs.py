@@ -30,8 +30,6 @@ import numpy as np
 
 from . import COMPONENTS, Simulation
 
-_RAW = {2: "int16", 4: "int32", 8: "int64"}  # raw containers for 2/4/8-byte storage
-
 
 class HaloPlan:
     """Owned and local z-ranges of each part, and the planes each exchange moves."""
@@ -109,19 +107,30 @@ def localize_sources(plan, r, sources):
     return out
 
 
+def _block_bytes(esz, nk, ny, nx):
+    """Bytes of nk planes of all six components; esz: bytes per value of each component."""
+    return sum(int(e) * nk * ny * nx for e in esz)
+
+
 def _block(sim, k0, nk, esz, device, stream):
-    """[6, nk, ny, nx] raw tensor of planes [k0, k0+nk) (local) of all components."""
+    """Flat uint8 tensor of planes [k0, k0+nk) (local) of the six components in their raw
+    storage format, one component after another (components may differ in size: f16e)."""
     import torch
     nx, ny, _ = sim.shape
-    buf = torch.empty((6, nk, ny, nx), dtype=getattr(torch, _RAW[esz]), device=device)
+    buf = torch.empty(_block_bytes(esz, nk, ny, nx), dtype=torch.uint8, device=device)
+    off = 0
     for c in range(6):
-        sim.get_planes_device(c, k0, nk, buf[c].data_ptr(), stream)
+        sim.get_planes_device(c, k0, nk, buf.data_ptr() + off, stream)
+        off += int(esz[c]) * nk * ny * nx
     return buf
 
 
-def _unblock(sim, k0, nk, buf, stream):
+def _unblock(sim, k0, nk, buf, esz, stream):
+    nx, ny, _ = sim.shape
+    off = 0
     for c in range(6):
-        sim.set_planes_device(c, k0, nk, buf[c].data_ptr(), stream)
+        sim.set_planes_device(c, k0, nk, buf.data_ptr() + off, stream)
+        off += int(esz[c]) * nk * ny * nx
 
 
 class ZSlabGrid:
@@ -140,7 +149,7 @@ class ZSlabGrid:
         self.sims = [Simulation(nx, ny, self.plan.local_nz(r), device=self.devices[r],
                                 kernel=kernel, blt=halo, tile_rows=tile_rows, storage=storage)
                      for r in range(parts)]
-        self.esz = self.sims[0].storage_bytes()
+        self.esz = [self.sims[0].component_bytes(c) for c in range(6)]
         self.monitors = []  # global id -> (part, local id)
         self.t = 0
 
@@ -181,7 +190,7 @@ class ZSlabGrid:
                 with torch.cuda.device(self.devices[peer]):
                     buf = buf.to(f"cuda:{self.devices[peer]}")
                     torch.cuda.synchronize(self.devices[peer])
-                    _unblock(dst, k0 - self.plan.loc[peer][0], nk, buf, None)
+                    _unblock(dst, k0 - self.plan.loc[peer][0], nk, buf, self.esz, None)
                     dst.sync()
 
     def step(self, T):
@@ -268,7 +277,7 @@ class DistZSlab:
         self.lo = self.plan.loc[self.rank][0]
         self.sim = Simulation(nx, ny, self.plan.local_nz(self.rank), device=self.device,
                               kernel=kernel, blt=halo, tile_rows=tile_rows, storage=storage)
-        self.esz = self.sim.storage_bytes()
+        self.esz = [self.sim.component_bytes(c) for c in range(6)]
         self.monitors = []
         self.t = 0
 
@@ -299,10 +308,10 @@ class DistZSlab:
             return _block(self.sim, k0 - self.lo, nk, self.esz, dev, stream)
 
         def put_block(k0, nk, buf):
-            _unblock(self.sim, k0 - self.lo, nk, buf, stream)
+            _unblock(self.sim, k0 - self.lo, nk, buf, self.esz, stream)
 
         def make_buffer(nk):
-            return torch.empty((6, nk, ny, nx), dtype=getattr(torch, _RAW[self.esz]), device=dev)
+            return torch.empty(_block_bytes(self.esz, nk, ny, nx), dtype=torch.uint8, device=dev)
 
         exchange_dist(self.plan, self.rank, get_block, put_block, make_buffer)
 

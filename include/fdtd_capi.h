@@ -69,15 +69,19 @@ typedef enum fdtd_kernel {
   FDTD_KERNEL_TILED_W32P = 5  /* tiled, an x-pair per thread, two 32-wide rows per warp */
 } fdtd_kernel;
 
-/* Field storage in HBM.  F32/F16/BF16 update in FP32 arithmetic; F16/BF16 store each
+/* Field storage in HBM.  F32/F16/BF16/F16E update in FP32 arithmetic; F16/BF16 store each
  * component with a per-component power-of-two scale (value = stored * scale) and run the tiled
- * x-pair kernel only.  F64 stores and updates in FP64 with the naive kernel: the error
- * reference for reduced-precision runs (coefficients and waveforms widened from FP32). */
+ * x-pair kernel only.  F16E stores the E components in FP16 (scaled) and the H components in
+ * FP32: 36 field bytes per cell-update instead of 24 (F16) or 48 (F32), and half of F16's
+ * storage roundings per pass.  F64 stores and updates in FP64 with the naive
+ * kernel: the error reference for reduced-precision runs (coefficients and waveforms widened
+ * from FP32).  The reference stores float fields only (gDiamond.h). */
 typedef enum fdtd_storage {
   FDTD_STORE_F32 = 0,
   FDTD_STORE_F16 = 1,
   FDTD_STORE_BF16 = 2,
-  FDTD_STORE_F64 = 3
+  FDTD_STORE_F64 = 3,
+  FDTD_STORE_F16E = 4
 } fdtd_storage;
 
 typedef struct fdtd_desc {
@@ -174,7 +178,7 @@ fdtd_status fdtd_get_dft_device(fdtd_handle* h, int32_t monitor_id, double* re_d
                                 double* im_dev, void* stream);
 /* Raw copies of the z-planes [k0, k0+nk) of one component of the current field set between the
  * handle and an unpitched device buffer of nk*Ny*Nx values in the storage format (esz bytes
- * each, fdtd_storage_bytes), on `stream` (NULL: the handle's stream; asynchronous).  The halo
+ * each, fdtd_component_bytes), on `stream` (NULL: the handle's stream; asynchronous).  The halo
  * exchange of a grid split into z-slabs (gdiamond_b200/slabs.py).  No reference counterpart:
  * gDiamond runs one grid on one GPU. */
 fdtd_status fdtd_get_planes_device(fdtd_handle* h, int32_t component, int64_t k0, int64_t nk,
@@ -182,12 +186,17 @@ fdtd_status fdtd_get_planes_device(fdtd_handle* h, int32_t component, int64_t k0
 fdtd_status fdtd_set_planes_device(fdtd_handle* h, int32_t component, int64_t k0, int64_t nk,
                                    const void* dev_in, void* stream);
 fdtd_status fdtd_storage_bytes(const fdtd_handle* h, int32_t* esz);
+/* Bytes per stored value of one component (0..5 = Ex Ey Ez Hx Hy Hz): differs from
+ * fdtd_storage_bytes only for F16E (2 for E, 4 for H); the raw plane copies above move values
+ * of this size.  No reference counterpart. */
+fdtd_status fdtd_component_bytes(const fdtd_handle* h, int32_t component, int32_t* esz);
 /* Device-to-device field copy into an unpitched Nx*Ny*Nz float array (asynchronous). */
 fdtd_status fdtd_get_field_device(fdtd_handle* h, int32_t component, float* dev_out,
                                   void* stream);
 
-/* Per-component storage scale for F16/BF16 storage (ignored otherwise); default 1.  Each scale
- * is rounded to the nearest power of two, so scaling never rounds. */
+/* Per-component storage scale for components stored in FP16/BF16 (ignored for FP32/FP64 ones,
+ * so F16E uses scale6[0..2] only); default 1.  Each scale is rounded to the nearest power of
+ * two, so scaling never rounds. */
 fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6);
 /* Field transfer into FP64 host memory (any storage; exact for F64 storage). */
 fdtd_status fdtd_get_field_f64(fdtd_handle* h, int32_t component, double* host_out);

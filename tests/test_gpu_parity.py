@@ -291,13 +291,13 @@ def test_gpu_coefficient_builder_matches_reference_formula(shape):
         sim2.close()
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "f64", "f16e"])
 def test_checkpoint_resume_continues_bit_for_bit(storage):
     """checkpoint() after 13 steps, restore() into a fresh handle, 11 more steps: the same
     fields and DFT sums as 24 uninterrupted steps.  16-bit storage rounds once per BLT-step
     pass, so there the split falls on a pass boundary (12 + 12: a multiple of every BLT the
     16-bit kernel uses); FP32 / FP64 split anywhere."""
-    first = 12 if storage == "f16" else 13
+    first = 12 if storage in ("f16", "f16e") else 13
     shape = (45, 33, 27)
     eps = W.spheres_eps(shape, n_spheres=3, r_range=(3, 6), seed=5)
     coefs = W.reference_coefficients(shape, eps_re=eps)
@@ -307,7 +307,7 @@ def test_checkpoint_resume_continues_bit_for_bit(storage):
 
     def make():
         sim = gd.Simulation(*shape, storage=storage)
-        if storage == "f16":
+        if storage in ("f16", "f16e"):
             sim.set_storage_scale([4.0] * 3 + [1.0] * 3)
         sim.set_coefficients(coefs)
         sim.set_sources(src)

@@ -1,10 +1,10 @@
 """Reduced-precision storage, FP64 storage and batches, on the GPU, against the oracle.
 
-* FP16 / BF16 storage: the tiled kernel computes each BLT-step pass in exact FP32 from the
-  stored (rounded) fields and rounds once when it writes the pass's result.  The oracle
-  reproduces that bit for bit: run BLT steps in FP32, then round every field to the storage
-  type (value * inv_scale rounded to nearest-even, read back times scale).  Monitors sum the
-  unrounded FP32 values in both.
+* FP16 / BF16 / F16E storage: the tiled kernel computes each BLT-step pass in exact FP32 from
+  the stored (rounded) fields and rounds once when it writes the pass's result.  The oracle
+  reproduces that bit for bit: run BLT steps in FP32, then round every field to its storage
+  type (value * inv_scale rounded to nearest-even, read back times scale; F16E rounds E to
+  FP16 and leaves H in FP32).  Monitors sum the unrounded FP32 values in both.
 * FP64 storage: the naive kernel in double against the oracle's FP64 stepper, bit for bit.
 * Batches: uneven grids with their own materials, sources and monitors advanced together by
   the persistent kernel (with and without CUDA-graph replay) against the oracle.
@@ -33,10 +33,13 @@ def round_bf16(x):
 def storage_roundtrip(F, storage, scales):
     out = []
     for c, f in enumerate(F):
+        if storage == "f16e" and c >= 3:  # H in FP32: no rounding, no scale
+            out.append(np.asarray(f, np.float32).copy())
+            continue
         sc = np.float32(scales[c])
         inv = np.float32(1.0) / sc
         v = (np.asarray(f, np.float32) * inv).astype(np.float32)
-        if storage == "f16":
+        if storage in ("f16", "f16e"):
             r = v.astype(np.float16).astype(np.float32)
         else:
             r = round_bf16(v)
@@ -72,7 +75,7 @@ def osrc(s):
                          kind=s.get("kind", 0))
 
 
-@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("storage", ["f16", "bf16", "f16e"])
 @pytest.mark.parametrize("blt,rows", [(2, 16), (3, 8), (4, 16)])
 def test_16bit_storage_matches_rounded_oracle(storage, blt, rows):
     shape, T = (70, 41, 33), 14
@@ -98,7 +101,7 @@ def test_16bit_storage_matches_rounded_oracle(storage, blt, rows):
     assert np.array_equal(re, omons[0].re) and np.array_equal(im, omons[0].im)
 
 
-@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("storage", ["f16", "bf16", "f16e"])
 @pytest.mark.parametrize("blt,rows", [(1, 48), (2, 32), (2, 48), (3, 32)])
 def test_16bit_pairs32_matches_rounded_oracle(storage, blt, rows):
     """The x-pair kernel with 32-cell rows (two per warp) and 16-bit storage."""
@@ -125,8 +128,11 @@ def test_16bit_pairs32_matches_rounded_oracle(storage, blt, rows):
 
 
 def test_16bit_rejects_naive_and_accepts_power_of_two_scales():
-    with pytest.raises(gd.FdtdError):
-        gd.Simulation(20, 20, 20, storage="f16", kernel="naive")
+    for storage in ("f16", "f16e"):
+        with pytest.raises(gd.FdtdError):
+            gd.Simulation(20, 20, 20, storage=storage, kernel="naive")
+        with pytest.raises(gd.FdtdError):
+            gd.Simulation(20, 20, 20, storage=storage, kernel="tiled_w32")
     sim = gd.Simulation(40, 30, 20, storage="bf16")
     with pytest.raises(gd.FdtdError):
         sim.set_storage_scale([1, 1, 1, 1, 0, 1])
@@ -135,6 +141,23 @@ def test_16bit_rejects_naive_and_accepts_power_of_two_scales():
     sim.set_field("Ex", x)
     got = sim.get_field("Ex")
     assert np.array_equal(got, storage_roundtrip([x] * 6, "bf16", [4.0] * 6)[0])
+    sim.close()
+
+
+def test_f16e_stores_e_in_fp16_and_h_in_fp32():
+    shape = (40, 30, 20)
+    sim = gd.Simulation(*shape, storage="f16e")
+    assert sim.storage_bytes() == 2
+    assert [sim.component_bytes(c) for c in range(6)] == [2, 2, 2, 4, 4, 4]
+    sim.set_storage_scale([4.0] * 6)  # used by the FP16 (E) components only
+    x = np.linspace(-3, 3, 40 * 30 * 20).astype(np.float32)
+    for comp in gd.COMPONENTS:
+        sim.set_field(comp, x)
+    want = storage_roundtrip([x] * 6, "f16e", [4.0] * 6)
+    assert not np.array_equal(want[0], x)
+    for c, comp in enumerate(gd.COMPONENTS):
+        assert bits_equal(sim.get_field(comp), want[c]), comp
+    assert np.array_equal(sim.get_field_f64(5), x.astype(np.float64))
     sim.close()
 
 
@@ -209,16 +232,18 @@ def test_batch_fp32_matches_oracle_and_replays(use_graph):
         sim.close()
 
 
-def test_batch_bf16_matches_rounded_oracle():
+@pytest.mark.parametrize("storage", ["bf16", "f16e"])
+def test_batch_16bit_matches_rounded_oracle(storage):
     T = 15
     scales = [8.0, 8.0, 8.0, 2.0, 2.0, 0.5]
-    sims, refs = make_batch("bf16", T, scales)
+    sims, refs = make_batch(storage, T, scales)
     batch = gd.Batch(sims)
     batch.step(T)
     blt = batch.config()["blt"]
     for sim, (shape, coefs, src, mons) in zip(sims, refs):
         omons = [oracle.Monitor(m["component"], m["k"], m["freqs"], m["scale"]) for m in mons]
-        F_ref = oracle_stored(shape, coefs, T, blt, "bf16", scales, [osrc(s) for s in src], omons)
+        F_ref = oracle_stored(shape, coefs, T, blt, storage, scales, [osrc(s) for s in src],
+                              omons)
         sim.sync()
         for c, f in enumerate(sim.fields()):
             assert bits_equal(f, F_ref[c]), (shape, oracle.COMPONENTS[c])

@@ -1,7 +1,8 @@
 """One grid run as z-slabs on the GPU (gdiamond_b200/slabs.py ZSlabGrid): several handles on one
 device, halo exchange through fdtd_get/set_planes_device after every BLT-step launch, against
-the same grid run as one handle with the same BLT -- bit for bit, fields and DFT sums, for FP32
-and BF16 storage (the exchange moves stored values raw), with a short last block.
+the same grid run as one handle with the same BLT -- bit for bit, fields and DFT sums, for FP32,
+BF16 and F16E storage (the exchange moves stored values raw; F16E's E and H components differ
+in size), with a short last block.
 """
 import numpy as np
 import pytest
@@ -27,7 +28,7 @@ def problem(T):
     return coefs, sources, freqs
 
 
-@pytest.mark.parametrize("storage", ["f32", "bf16"])
+@pytest.mark.parametrize("storage", ["f32", "bf16", "f16e"])
 @pytest.mark.parametrize("parts,halo,T", [(3, 2, 31), (2, 3, 20), (4, 1, 9)])
 def test_slabs_match_single_grid(storage, parts, halo, T):
     coefs, sources, freqs = problem(T)
