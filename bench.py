@@ -335,11 +335,13 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
                      "note": f"achieved = {B_ALG} B/cell-update x {cells_per_launch} cell-updates "
-                             f"per launch / mean launch time {launch_ms:.4f} ms; peak {kind}; "
+                             f"per launch / mean launch time {launch_ms:.4f} ms (step time / "
+                             f"{launches_per_step} tiled launches; the step's "
+                             f"{cfg['dft_folds']} DFT folds included); peak {kind}; "
                              f"temporal tiling lets frac exceed 1"},
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": launches_per_step * args.steps,
+        "gpu_launches": (launches_per_step + cfg["dft_folds"]) * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line))

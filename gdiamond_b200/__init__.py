@@ -41,6 +41,7 @@ EXPORTS = (
     "fdtd_mlp_train", "fdtd_mlp_predict", "fdtd_mlp_predict_device", "fdtd_get_dft_device",
     "fdtd_mlp_set_gemm", "fdtd_get_planes_device", "fdtd_set_planes_device",
     "fdtd_storage_bytes", "fdtd_set_step", "fdtd_set_dft", "fdtd_component_bytes",
+    "fdtd_dft_folds",
 )
 
 
@@ -101,6 +102,7 @@ def library():
             "fdtd_set_planes_device": ([V, C.c_int32, C.c_int64, C.c_int64, V, V], C.c_int),
             "fdtd_storage_bytes": ([V, P(C.c_int32)], C.c_int),
             "fdtd_component_bytes": ([V, C.c_int32, P(C.c_int32)], C.c_int),
+            "fdtd_dft_folds": ([V, P(C.c_int32)], C.c_int),
             "fdtd_set_step": ([V, C.c_int64], C.c_int),
             "fdtd_set_dft": ([V, C.c_int32, P(C.c_double), P(C.c_double)], C.c_int),
             "fdtd_batch_create": ([P(V), C.c_int32, P(V)], C.c_int),
@@ -289,9 +291,11 @@ class Simulation:
         self._check(self._L.fdtd_get_config(self._h, out))
         kernel = {1: "naive", 3: "tiled", 4: "tiled", 5: "tiled"}.get(out[0], "none")
         width = {3: 32, 4: 64, 5: 32}.get(out[0], 0)
+        folds = C.c_int32()
+        self._check(self._L.fdtd_dft_folds(self._h, C.byref(folds)))
         return {"kernel": kernel, "width": width, "pairs": out[0] in (4, 5), "blt": out[1],
                 "tile_rows": out[2], "z_chunks": out[3], "launches": out[4],
-                "min_blocks": out[5]}
+                "min_blocks": out[5], "dft_folds": folds.value}
 
     # ---------------------------------------------------------------- results
     def get_field(self, component, out=None):
@@ -447,8 +451,10 @@ class Batch:
     def config(self):
         out = (C.c_int32 * 6)()
         self._check(self._L.fdtd_batch_get_config(self._h, out))
+        folds = C.c_int32()
+        self._check(self._L.fdtd_dft_folds(self.sims[0]._h, C.byref(folds)))
         return {"blt": out[0], "tile_rows": out[1], "ctas": out[2], "items": out[3],
-                "launches": out[4], "graph_replayed": bool(out[5])}
+                "launches": out[4], "graph_replayed": bool(out[5]), "dft_folds": folds.value}
 
     def close(self):
         if getattr(self, "_h", None):

@@ -42,6 +42,7 @@ struct MonitorHost {
   double* im = nullptr;
   double2* tab = nullptr;  // [tab_cap][nf]
   long long tab_cap = 0;
+  float* stage = nullptr;  // [kDftSlots][ny][nx]: values the tiled kernels stage for the fold
 };
 
 std::string g_create_error;
@@ -93,6 +94,7 @@ struct fdtd_handle {
   CUtensorMap mat_map;
   int maps_key = 0;  // width * 1000 + rows of the encoded boxes
   int last_kernel = 0, last_launches = 0;
+  int last_folds = 0;  // DFT fold launches of the last fdtd_step
   int storage = FDTD_STORE_F32;
   int esz = 4;     // bytes per stored field value (F16E: the FP16 E components')
   int nsets = 2;   // field sets (1 for FP64: the naive kernel updates in place)
@@ -222,6 +224,7 @@ fdtd::Monitors make_monitors(const fdtd_handle* h) {
     M.m[m].tab = mh.tab;
     M.m[m].re = mh.re;
     M.m[m].im = mh.im;
+    M.m[m].stage = mh.stage;
   }
   return M;
 }
@@ -420,6 +423,7 @@ void free_all(fdtd_handle* h) {
     cudaFree(h->mon[m].re);
     cudaFree(h->mon[m].im);
     cudaFree(h->mon[m].tab);
+    cudaFree(h->mon[m].stage);
   }
   if (h->stream) cudaStreamDestroy(h->stream);
 }
@@ -718,6 +722,9 @@ fdtd_status fdtd_add_dft_monitor(fdtd_handle* h, int32_t component, int64_t k,
   CUDA_TRY(h, cudaMalloc(&m.im, bytes));
   CUDA_TRY(h, cudaMemsetAsync(m.re, 0, bytes, h->stream));
   CUDA_TRY(h, cudaMemsetAsync(m.im, 0, bytes, h->stream));
+  const size_t stage_bytes = (size_t)fdtd::kDftSlots * h->g.nx * h->g.ny * sizeof(float);
+  CUDA_TRY(h, cudaMalloc(&m.stage, stage_bytes));
+  CUDA_TRY(h, cudaMemsetAsync(m.stage, 0, stage_bytes, h->stream));
   if (monitor_id) *monitor_id = h->nmon;
   h->nmon += 1;
   return FDTD_OK;
@@ -766,7 +773,7 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
     return fail(h, FDTD_ERR_UNSUPPORTED,
                 "the tiled kernel needs a material map (more than %d distinct coefficient "
                 "tuples were given)", kMaxMaterials);
-  int launches = 0;
+  int launches = 0, folds = 0;
   const fdtd::Sources S = make_sources(h);
   const fdtd::Monitors M = make_monitors(h);
   if (kernel == FDTD_KERNEL_NAIVE) {
@@ -790,12 +797,21 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
     c.esz = h->esz;
     s = ensure_maps(h, c.width, c.rows);
     if (s != FDTD_OK) return s;
+    // The tiled kernels stage monitor-plane values in a ring of kDftSlots steps; a fold adds
+    // them to the sums before the ring would wrap and once more at the end, so the sums are
+    // complete whenever fdtd_step returns.
+    long long t_fold = h->t;
     int64_t left = T;
     while (left > 0) {
       fdtd::TiledConfig cc = c;
       if (left < c.blt) {  // a shorter final pass (plain register allocation)
         cc.blt = (int)left;
         cc.min_blocks = 1;
+      }
+      if (M.n > 0 && h->t + cc.blt - t_fold > fdtd::kDftSlots) {
+        CUDA_TRY(h, fdtd::launch_dft_fold(M, h->g, t_fold, (int)(h->t - t_fold), st));
+        ++folds;
+        t_fold = h->t;
       }
       const fdtd::TiledArgs a = make_tiled_args(h, cc, h->t, true);
       CUDA_TRY(h, launch_any(cc, a, h->g, st));
@@ -804,10 +820,15 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
       h->t += cc.blt;
       left -= cc.blt;
     }
+    if (M.n > 0 && h->t > t_fold) {
+      CUDA_TRY(h, fdtd::launch_dft_fold(M, h->g, t_fold, (int)(h->t - t_fold), st));
+      ++folds;
+    }
     h->last_kernel = c.pairs32 ? FDTD_KERNEL_TILED_W32P
                                : (c.width == 64 ? FDTD_KERNEL_TILED_W64 : FDTD_KERNEL_TILED_W32);
   }
   h->last_launches = launches;
+  h->last_folds = folds;
   if (st != h->stream) {
     cudaEvent_t ev;
     CUDA_TRY(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -1009,6 +1030,12 @@ fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6) {
   return FDTD_OK;
 }
 
+fdtd_status fdtd_dft_folds(const fdtd_handle* h, int32_t* n) {
+  if (!h || !n) return FDTD_ERR_INVALID_ARG;
+  *n = h->last_folds;
+  return FDTD_OK;
+}
+
 fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out6) {
   if (!h || !out6) return FDTD_ERR_INVALID_ARG;
   out6[0] = h->last_kernel;
@@ -1044,7 +1071,8 @@ struct fdtd_batch {
   int ctas = 0;
   cudaGraphExec_t gexec = nullptr;
   std::vector<long long> gkey;
-  int last_launches = 0, last_graph = 0;
+  int gfolds = 0;  // DFT fold launches in the captured graph
+  int last_launches = 0, last_graph = 0, last_folds = 0;
   std::string err;
 };
 
@@ -1325,23 +1353,50 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
   if (rem && (s = batch_items(b, batch_cfg(b, rem, c.rows, c.pairs32), &tmp)) != FDTD_OK)
     return s;
   batch_fill_args(b, c, true);
+  // Deferred DFT: the largest monitor plane and frequency count size the fold launches.
+  long long max_np = 0;
+  int max_nf = 0;
+  for (fdtd_handle* h : b->sims)
+    for (int m = 0; m < h->nmon; ++m) {
+      max_np = std::max<long long>(max_np, (long long)h->g.nx * h->g.ny);
+      max_nf = std::max(max_nf, h->mon[m].nf);
+    }
+  int folds = 0;
 
+  // Monitor values staged by the batched kernel are folded into the sums before a ring of
+  // kDftSlots steps would wrap and at the end (the grids' t0 in d_args parity 0 is their step
+  // counter at the start of this call).
   auto record = [&](cudaStream_t rs) -> fdtd_status {
     BCUDA(b, cudaMemcpyAsync(b->d_args, b->h_args,
                              2 * b->sims.size() * sizeof(fdtd::TiledArgs),
                              cudaMemcpyHostToDevice, rs));
     BCUDA(b, cudaMemsetAsync(b->d_counters, 0, nl * sizeof(unsigned int), rs));
+    const int ng = (int)b->sims.size();
+    long long folded = 0;
+    folds = 0;
     for (int k = 0; k < nl; ++k) {
       const fdtd::TiledConfig ck = (k < nfull) ? c : batch_cfg(b, rem, c.rows, c.pairs32);
-      fdtd_status r = batch_launch(b, ck, k & 1, (long long)k * c.blt, b->d_counters + k, rs);
+      const long long off = (long long)k * c.blt;
+      if (max_nf > 0 && off + ck.blt - folded > fdtd::kDftSlots) {
+        BCUDA(b, fdtd::launch_dft_fold_batch(b->d_args, ng, max_np, max_nf, folded,
+                                             (int)(off - folded), rs));
+        ++folds;
+        folded = off;
+      }
+      fdtd_status r = batch_launch(b, ck, k & 1, off, b->d_counters + k, rs);
       if (r != FDTD_OK) return r;
+    }
+    if (max_nf > 0 && T > folded) {
+      BCUDA(b, fdtd::launch_dft_fold_batch(b->d_args, ng, max_np, max_nf, folded,
+                                           (int)(T - folded), rs));
+      ++folds;
     }
     return FDTD_OK;
   };
 
   b->last_graph = 0;
   if (use_graph) {
-    std::vector<long long> key = {T, c.blt, c.rows, b->ctas, b->zlen};
+    std::vector<long long> key = {T, c.blt, c.rows, b->ctas, b->zlen, max_np, max_nf};
     for (fdtd_handle* h : b->sims) {
       key.push_back(h->t);
       key.push_back(h->cur);
@@ -1363,8 +1418,10 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
       if (ce != cudaSuccess) return bfail(b, FDTD_ERR_CUDA, "graph instantiation failed: %s",
                                           cudaGetErrorString(ce));
       b->gkey = key;
+      b->gfolds = folds;
     } else {
       b->last_graph = 1;
+      folds = b->gfolds;
     }
     BCUDA(b, cudaGraphLaunch(b->gexec, st));
   } else {
@@ -1378,9 +1435,11 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
     h->cur ^= (nl & 1);
     h->last_kernel = c.pairs32 ? FDTD_KERNEL_TILED_W32P : FDTD_KERNEL_TILED_W64;
     h->last_launches = nl;
+    h->last_folds = folds;
     if ((s = stream_after(b, h->stream, st)) != FDTD_OK) return s;
   }
   b->last_launches = nl;
+  b->last_folds = folds;
   return FDTD_OK;
 }
 

@@ -14,6 +14,9 @@ namespace fdtd {
 constexpr int kMaxSources = 8;
 constexpr int kMaxMonitors = 4;
 constexpr int kMaxFreqs = 64;
+// Steps a monitor's staging ring holds between folds (a power of two): the tiled kernels write
+// each monitor-plane value there, and a fold adds a window of them to the FP64 sums.
+constexpr int kDftSlots = 128;
 
 // Device error word values.
 constexpr int kErrNone = 0;
@@ -46,6 +49,7 @@ struct MonitorDev {
   const double2* tab;  // [t][nf] (cos, sin) of ph = (2*pi*f) * (t*dt)
   double* re;          // [nf][ny][nx]
   double* im;
+  float* stage;        // [kDftSlots][ny][nx] plane values of steps not yet folded (or null)
 };
 
 struct Monitors {
@@ -120,6 +124,19 @@ __device__ __forceinline__ void dft_accumulate(const MonitorDev& m, long long t,
     double* im = m.im + f * np + p;
     *re = dadd(*re, dmul(dmul(v, cs.x), m.scale));
     *im = dsub(*im, dmul(dmul(v, cs.y), m.scale));
+  }
+}
+
+// Monitor-plane value of step t at cell (i, j): into slot t % kDftSlots of the staging ring,
+// to be folded into the sums later in step order (dft_fold.cu), or straight into the sums
+// when the monitor has no ring.  Both give the same FP64 sums bit for bit.
+__device__ __forceinline__ void dft_record(const MonitorDev& m, long long t, int i, int j,
+                                           const Grid& g, float value) {
+  if (m.stage) {
+    const long long np = (long long)g.nx * g.ny;
+    m.stage[(t & (kDftSlots - 1)) * np + i + (long long)j * g.nx] = value;
+  } else {
+    dft_accumulate(m, t, i, j, g, value);
   }
 }
 

@@ -105,6 +105,16 @@ dim3 tiled_grid(const TiledConfig& c, const Grid& g);
 cudaError_t launch_tiled(const TiledConfig& c, const TiledArgs& args, const Grid& g,
                          cudaStream_t st);
 
+// ---------------------------------------------------------------- deferred DFT (dft_fold.cu)
+// Adds steps [t0, t0+n) (n <= kDftSlots) staged in the monitors' rings to their FP64 sums.
+cudaError_t launch_dft_fold(const Monitors& M, const Grid& g, long long t0, int n,
+                            cudaStream_t st);
+// The same for every grid of a batch: grids[0..ngrids) (device memory) with their monitors; the
+// window of grid i starts at grids[i].t0 + t_offset.  max_np / max_nf: the largest monitor
+// plane (Nx*Ny) and frequency count over the batch (grid size of the launch).
+cudaError_t launch_dft_fold_batch(const TiledArgs* grids, int ngrids, long long max_np,
+                                  int max_nf, long long t_offset, int n, cudaStream_t st);
+
 // ---------------------------------------------------------------- coefficient builder
 struct Coef12Out {
   float* c[12];  // pitched per-cell arrays Cax..Dbz

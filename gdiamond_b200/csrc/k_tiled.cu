@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(32 * TY) fdtd_tiled(const __grid_constant__ Ti
           const MonitorDev& m = a.M.m[n];
           const int mk = m.comp < 3 ? e : e - 1;
           if (m.k == mk && mk >= z0 && mk < z1)
-            dft_accumulate(m, t, x, y, g, m.comp < 3 ? pick3(En, m.comp) : pick3(Hn, m.comp - 3));
+            dft_record(m, t, x, y, g, m.comp < 3 ? pick3(En, m.comp) : pick3(Hn, m.comp - 3));
         }
       }
       // ---------------- exchange

@@ -358,8 +358,8 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
             const int c = m.comp < 3 ? m.comp : m.comp - 3;
             const Pair v = m.comp < 3 ? (c == 0 ? En[0] : (c == 1 ? En[1] : En[2]))
                                       : (c == 0 ? Hn[0] : (c == 1 ? Hn[1] : Hn[2]));
-            if (out0) dft_accumulate(m, t, x0, y, g, v.a);
-            if (out1) dft_accumulate(m, t, x1, y, g, v.b);
+            if (out0) dft_record(m, t, x0, y, g, v.a);
+            if (out1) dft_record(m, t, x1, y, g, v.b);
           }
         }
       }

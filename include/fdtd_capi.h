@@ -203,8 +203,14 @@ fdtd_status fdtd_get_field_f64(fdtd_handle* h, int32_t component, double* host_o
 
 /* Kernel configuration actually used by the last fdtd_step: out = {kernel, blt, tile_rows,
  * z_chunks, launches in the last fdtd_step, min_blocks}; kernel is FDTD_KERNEL_NAIVE,
- * _TILED_W32 or _TILED_W64. */
+ * _TILED_W32, _TILED_W64 or _TILED_W32P. */
 fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out6);
+/* DFT fold launches of the last fdtd_step or fdtd_batch_step that advanced h.  The tiled
+ * kernels stage monitor-plane values in a ring of 128 steps per monitor and a fold kernel adds
+ * them to the FP64 sums (bit-identical to accumulating every step) before the ring wraps and
+ * at the end of the call, so the sums are complete when the step call's work has run.  No
+ * reference counterpart: gDiamond accumulates its monitors with one kernel per step. */
+fdtd_status fdtd_dft_folds(const fdtd_handle* h, int32_t* n);
 
 /* Builds a material map from 12 device coefficient arrays without allocating anything.
  * No counterpart in the reference (which keeps 12 per-cell arrays); it is the allocation-free

@@ -154,6 +154,50 @@ def test_plane_source_random_eps_and_monitors(kernel):
     del rng
 
 
+def expected_folds(T, blt, slots=128):
+    """Fold launches of one step call: before a launch that would overrun the staging ring,
+    and once at the end."""
+    t = t_fold = n = 0
+    while t < T:
+        b = min(blt, T - t)
+        if t + b - t_fold > slots:
+            n, t_fold = n + 1, t
+        t += b
+    return n + (1 if T > t_fold else 0)
+
+
+@pytest.mark.parametrize("kernel,blt", [("tiled_w64", 2), ("tiled_w64", 3), ("tiled_w32", 5),
+                                        ("tiled_w32p", 2)])
+def test_dft_folds_across_ring_wraps(kernel, blt):
+    """The tiled kernels stage monitor values in a 128-step ring that a fold kernel adds to the
+    FP64 sums: 300 steps in one call (two wraps and a partial window) and in uneven calls
+    (130 + 1 + 169) give the oracle's sums bit for bit."""
+    shape, T = (40, 34, 26), 300
+    coefs = W.reference_coefficients(shape)
+    w = W.gaussian_wave(T, delay=30.0, width=10.0, period=12.0)
+    src = [dict(component="Jz", wave=w, i=20, j=17, k=13)]
+    freqs = W.source_band(11, period=12.0, width=10.0)
+    mons = [dict(component="Ez", k=15, freqs=freqs, scale=1.0),
+            dict(component="Hy", k=9, freqs=freqs[:3], scale=0.5)]
+    omons = [oracle.Monitor(m["component"], m["k"], m["freqs"], m["scale"]) for m in mons]
+    F_ref = oracle.run(shape, coefs, T, sources=[osrc(s) for s in src], monitors=omons)
+    sim = gd.Simulation(*shape, kernel=kernel, blt=blt)
+    sim.set_coefficients(coefs)
+    sim.set_sources(src)
+    mids = [sim.add_dft_monitor(m["component"], m["k"], m["freqs"], m["scale"]) for m in mons]
+    for calls in ((T,), (130, 1, 169)):
+        sim.reset()
+        for n in calls:
+            sim.step(n)
+        assert sim.config()["dft_folds"] == expected_folds(calls[-1], blt)
+        assert_fields_match(sim.fields(), F_ref, f"{kernel} {calls}")
+        for mid, om in zip(mids, omons):
+            re, im = sim.get_dft(mid)
+            assert np.abs(om.re).max() > 0
+            assert np.array_equal(re, om.re) and np.array_equal(im, om.im), (kernel, calls, mid)
+    sim.close()
+
+
 def test_per_cell_coefficients_fall_back_to_naive():
     shape, T = (48, 40, 44), 20  # 84480 cells, almost all with their own 12-tuple (> 65536)
     n = int(np.prod(shape))
