@@ -563,7 +563,7 @@ def run_batched(args):
 
 
 def run_surrogate(args):
-    """Learned surrogate: 4096 training + 512 held-out designs (a dielectric box in a 96^3
+    """Learned surrogate: 16384 training + 512 held-out designs (a dielectric box in a 96^3
     grid, six numbers each), transmission spectra at 64 frequencies from the batched FP32 solver
     (CUDA graph, T=2000); an ensemble of 4 MLPs 6->256->256->256->64 trained on the GPU
     (BF16 tensor-core GEMMs, FP32 accumulation, Adam lr 1e-3, 200 epochs); held-out spectral
@@ -743,7 +743,7 @@ def main():
                     help="batched workload: storages of the batched runs")
     ap.add_argument("--designs", type=int, default=1 << 20, help="mlp: designs per inference")
     ap.add_argument("--train-epochs", type=int, default=10, help="mlp: timed training epochs")
-    ap.add_argument("--train", type=int, default=4096, help="surrogate: training designs")
+    ap.add_argument("--train", type=int, default=16384, help="surrogate: training designs")
     ap.add_argument("--test", type=int, default=512, help="surrogate: held-out designs")
     ap.add_argument("--epochs", type=int, default=200, help="surrogate: training epochs")
     ap.add_argument("--mlp-batch", type=int, default=64, help="surrogate: minibatch rows")
