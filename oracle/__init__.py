@@ -104,8 +104,17 @@ def ref():
         L.gdref_get_fields.restype = C.c_int
         L.gdref_get_fields.argtypes = [C.c_void_p, C.c_int, P(P(C.c_float))]
         L.gdref_max_threads.restype = C.c_int
+        L.gdref_save_field_png.argtypes = [P(C.c_float), C.c_char_p, C.c_int, C.c_int,
+                                           C.c_float]
         _ref = L
     return _ref
+
+
+def ref_save_field_png(u, path, vmax):
+    """The reference's save_field_png (gDiamond/utils.h:210-255) on a [ny][nx] float32 slice."""
+    u = np.ascontiguousarray(u, np.float32)
+    ny, nx = u.shape
+    ref().gdref_save_field_png(_fptr(u), os.fsencode(path), nx, ny, float(vmax))
 
 
 def _fptr(a: np.ndarray, T=C.c_float):

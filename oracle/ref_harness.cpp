@@ -10,6 +10,7 @@
 //   gdiamond::gDiamond::update_FDTD_seq(T)        gDiamond/gdiamond.hpp:1164-1263
 //   gdiamond::gDiamond::update_FDTD_omp(T)        gDiamond/gdiamond_omp.hpp:110-172
 //   gdiamond::gDiamond::update_FDTD_omp_dt(...)   gDiamond/gdiamond_omp.hpp:174-261
+//   save_field_png(u, filename, Nx, Ny, vmax)     gDiamond/utils.h:210-255
 //
 // Two harness workarounds (both needed to run the reference as shipped):
 //   1. the standard headers are included before `#define private public`, which otherwise
@@ -131,5 +132,10 @@ int gdref_get_fields(void* h, int variant, float* const* out6) {
 }
 
 int gdref_max_threads(void) { return omp_get_max_threads(); }
+
+// The reference's field-slice PNG writer (blue-white-red map clipped to +-vmax).
+void gdref_save_field_png(const float* u, const char* filename, int nx, int ny, float vmax) {
+  save_field_png(const_cast<float*>(u), filename, nx, ny, vmax);
+}
 
 }  // extern "C"

@@ -9,9 +9,13 @@ stores their outputs:
 * ``ref_seq_24x20x16_T30.npz`` -- the same for 24 x 20 x 16, 30 steps;
 * ``ref_100cube_T100.json`` -- the reference unit-test configuration (100^3 cells, 100 steps,
   unittests/checker_*.cpp): per-component L2 norm and SHA-256 of the FP32 field bytes of seq,
-  omp and omp_dt(16,16,16,5), and SHA-256 of the 12 coefficient arrays.
+  omp and omp_dt(16,16,16,5), and SHA-256 of the 12 coefficient arrays;
+* ``ref_png_37x23.npz`` -- a seeded 37 x 23 field slice (values beyond +-vmax, zeros, -0.0
+  included), its vmax, and the PNG file the reference's save_field_png (utils.h:210-255) writes
+  for it, as bytes.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [small cube png]
+(no arguments: every fixture).
 """
 import hashlib
 import json
@@ -61,10 +65,28 @@ def cube():
         json.dump(res, f, indent=1, sort_keys=True)
 
 
+def png():
+    import tempfile
+    rng = np.random.default_rng(21)
+    u = (rng.standard_normal((23, 37)) * 1.5).astype(np.float32)
+    u[0, :5] = [0.0, -0.0, 2.0, -2.0, 1e-30]
+    vmax = np.float32(2.0)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "slice.png")
+        oracle.ref_save_field_png(u, path, vmax)
+        data = np.frombuffer(open(path, "rb").read(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "ref_png_37x23.npz"), u=u, vmax=vmax, png=data)
+
+
 if __name__ == "__main__":
     if not oracle.ref_available():
         oracle.build()
-    small((17, 13, 11), 25)
-    small((24, 20, 16), 30)
-    cube()
+    which = set(sys.argv[1:]) or {"small", "cube", "png"}
+    if "small" in which:
+        small((17, 13, 11), 25)
+        small((24, 20, 16), 30)
+    if "cube" in which:
+        cube()
+    if "png" in which:
+        png()
     print("golden fixtures written to", HERE)
