@@ -17,9 +17,9 @@
 //    inner (32-2*BLT) x (ROWS-2*BLT) cells of level BLT.  x tile starts are multiples of 4
 //    elements (16-byte TMA rule).
 //  * Coefficients come from a per-material table indexed by the uint16 map (2 bytes per cell
-//    instead of 48).  Sources are a short descriptor list; DFT monitors on z-planes accumulate
-//    in FP64 when a level passes the monitor plane, inside the same tile, so no extra field
-//    pass is made.
+//    instead of 48).  Sources are a short descriptor list.  When a level passes a DFT monitor
+//    plane the tile writes that step's values into the monitor's staging ring (dft_record), so
+//    no extra field pass is made; dft_fold.cu adds the ring to the FP64 sums.
 //  * Source set -> destination set (ping-pong), so overlapping tiles never see each other's
 //    writes.  Every multiply/add is separately rounded: results are bit-identical to the
 //    reference CPU update.
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(32 * TY) fdtd_tiled(const __grid_constant__ Ti
         Hn[1] = yee(mc.x, Hp[s - 1][1], mc.y, cy);
         Hn[2] = yee(mc.z, Hp[s - 1][2], mc.w, cz);
       }
-      // ---------------- running DFT when this level passes a monitor plane
+      // ---------------- DFT monitors: stage this level's values when it passes a monitor plane
       if (mon_iter && col_out) {
         for (int n = 0; n < a.M.n; ++n) {
           const MonitorDev& m = a.M.m[n];

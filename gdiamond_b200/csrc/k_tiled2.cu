@@ -3,8 +3,8 @@
 // (fdtd_tiled2_batch), with 64-cell rows (one per warp) or 32-cell rows (two per warp).
 //
 // Same schedule as k_tiled.cu (TMA plane pipeline, BLT-level (z,t) wavefront, trapezoid tiles in
-// x and y, material map, fused FP64 DFT, bounded waits), but each thread owns an x-pair
-// (2l, 2l+1) of a 64-wide warp row:
+// x and y, material map, monitor values staged for the deferred DFT, bounded waits), but each
+// thread owns an x-pair (2l, 2l+1) of a 64-wide warp row:
 //  * the pair's inner neighbours are in registers; only the pair edges cross lanes, so a level
 //    needs one shuffle per field direction per pair instead of per cell;
 //  * staged planes, y-exchange planes and outputs move as pairs (one shared/global instruction
@@ -349,7 +349,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
           Hn[2].b = yee(c1.z, Hp[s - 1][2].b, c1.w, czp.b);
         }
       }
-      // ---------------- running DFT (of the FP32 values, before any storage rounding)
+      // ---------------- DFT monitors: stage the FP32 values (before any storage rounding)
       if (mon_iter && (out0 || out1)) {
         for (int n = 0; n < a.M.n; ++n) {
           const MonitorDev& m = a.M.m[n];
