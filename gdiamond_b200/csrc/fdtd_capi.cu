@@ -718,13 +718,21 @@ fdtd_status fdtd_add_dft_monitor(fdtd_handle* h, int32_t component, int64_t k,
   m.dt = dt;
   m.freqs.assign(freqs, freqs + nf);
   const size_t bytes = (size_t)nf * h->g.nx * h->g.ny * sizeof(double);
-  CUDA_TRY(h, cudaMalloc(&m.re, bytes));
-  CUDA_TRY(h, cudaMalloc(&m.im, bytes));
-  CUDA_TRY(h, cudaMemsetAsync(m.re, 0, bytes, h->stream));
-  CUDA_TRY(h, cudaMemsetAsync(m.im, 0, bytes, h->stream));
   const size_t stage_bytes = (size_t)fdtd::kDftSlots * h->g.nx * h->g.ny * sizeof(float);
-  CUDA_TRY(h, cudaMalloc(&m.stage, stage_bytes));
-  CUDA_TRY(h, cudaMemsetAsync(m.stage, 0, stage_bytes, h->stream));
+  cudaError_t e = cudaMalloc(&m.re, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&m.im, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&m.stage, stage_bytes);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m.re, 0, bytes, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m.im, 0, bytes, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m.stage, 0, stage_bytes, h->stream);
+  if (e != cudaSuccess) {  // the monitor is not added: release what it had
+    cudaFree(m.re);
+    cudaFree(m.im);
+    cudaFree(m.stage);
+    m = MonitorHost();
+    return fail(h, e == cudaErrorMemoryAllocation ? FDTD_ERR_OOM : FDTD_ERR_CUDA,
+                "monitor allocation failed: %s", cudaGetErrorString(e));
+  }
   if (monitor_id) *monitor_id = h->nmon;
   h->nmon += 1;
   return FDTD_OK;
