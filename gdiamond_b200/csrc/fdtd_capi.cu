@@ -291,7 +291,7 @@ std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
   const bool half = h->esz == 2;
   if (half) {
     fams = {1, 2};
-    rows_l = {8, 16, 32, 48};
+    rows_l = {8, 16, 24, 32, 48};
   }
   if (h->desc.blt > 0) blts = {h->desc.blt};
   if (h->desc.tile_rows > 0) rows_l = {h->desc.tile_rows};

@@ -476,9 +476,17 @@ __global__ void __launch_bounds__(TY * W / 2, MINB)
                                0);
 }
 
+// CTAs per SM the compiler must fit: two for the 24-row tiles of 32-cell rows (384 threads, the
+// register budget of the 48-row instance), one otherwise.
+template <int TY, int W>
+constexpr int batch_min_blocks() {
+  return (W == 32 && TY == 24) ? 2 : 1;
+}
+
 // A batch of independent grids: persistent CTAs pull (grid, tile) work items from a queue.
 template <typename S, int B, int TY, int W = 64, typename SH = S>
-__global__ void __launch_bounds__(TY * W / 2, 1) fdtd_tiled2_batch(const BatchArgs b) {
+__global__ void __launch_bounds__(TY * W / 2, (batch_min_blocks<TY, W>()))
+    fdtd_tiled2_batch(const BatchArgs b) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_abort;
   __shared__ int s_item;
@@ -517,10 +525,17 @@ cudaError_t launch_batch_one(const BatchArgs& b, int ctas, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// 32-wide rows (two per warp): 32 rows (16 warps, BLT 1-3) or 48 rows (24 warps, BLT 1-2).
+// 32-wide rows (two per warp): 24 rows (12 warps, BLT 1-2, registers capped for two CTAs per
+// SM), 32 rows (16 warps, BLT 1-3) or 48 rows (24 warps, BLT 1-2).
 template <typename S, typename SH = S>
 cudaError_t launch_pairs32(int blt, int rows, const TiledArgs& a, dim3 grid, cudaStream_t st) {
-  if (rows == 32) {
+  if (rows == 24) {
+    switch (blt) {
+      case 1: return launch_one2<S, 1, 24, 2, 32, SH>(a, grid, st);
+      case 2: return launch_one2<S, 2, 24, 2, 32, SH>(a, grid, st);
+      default: break;
+    }
+  } else if (rows == 32) {
     switch (blt) {
       case 1: return launch_one2<S, 1, 32, 1, 32, SH>(a, grid, st);
       case 2: return launch_one2<S, 2, 32, 1, 32, SH>(a, grid, st);
@@ -540,7 +555,13 @@ cudaError_t launch_pairs32(int blt, int rows, const TiledArgs& a, dim3 grid, cud
 template <typename S, typename SH = S>
 cudaError_t launch_batch_pairs32(int blt, int rows, const BatchArgs& b, int ctas,
                                  cudaStream_t st) {
-  if (rows == 32) {
+  if (rows == 24) {
+    switch (blt) {
+      case 1: return launch_batch_one<S, 1, 24, 32, SH>(b, ctas, st);
+      case 2: return launch_batch_one<S, 2, 24, 32, SH>(b, ctas, st);
+      default: break;
+    }
+  } else if (rows == 32) {
     switch (blt) {
       case 1: return launch_batch_one<S, 1, 32, 32, SH>(b, ctas, st);
       case 2: return launch_batch_one<S, 2, 32, 32, SH>(b, ctas, st);
@@ -658,7 +679,8 @@ int occupancy_of() {
 
 bool pairs32_supported(const TiledConfig& c) {
   return (c.esz == 4 || c.esz == 2) && c.width == 32 && c.min_blocks == 1 &&
-         ((c.rows == 32 && c.blt >= 1 && c.blt <= 3) || (c.rows == 48 && c.blt >= 1 && c.blt <= 2));
+         ((c.rows == 32 && c.blt >= 1 && c.blt <= 3) ||
+          ((c.rows == 24 || c.rows == 48) && c.blt >= 1 && c.blt <= 2));
 }
 
 // Shared memory (SMEM) or resident batch CTAs per SM (OCC) of the batch instance for config c.
@@ -667,7 +689,12 @@ size_t batch_query(const TiledConfig& c) {
 #define GD_Q(B, TY, W) (OCC ? (size_t)occupancy_of<S, B, TY, W, SH>() : smem_of<S, B, TY, W, SH>())
   constexpr bool f32 = sizeof(S) == 4 && sizeof(SH) == 4;
   if (c.pairs32) {
-    if (c.rows == 32) {
+    if (c.rows == 24) {
+      switch (c.blt) {
+        case 1: return GD_Q(1, 24, 32);
+        case 2: return GD_Q(2, 24, 32);
+      }
+    } else if (c.rows == 32) {
       switch (c.blt) {
         case 1: return GD_Q(1, 32, 32);
         case 2: return GD_Q(2, 32, 32);

@@ -105,7 +105,7 @@ CONFIGS += [(b, r, z, "tiled_w64") for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 
                                                 (20, (1, 2, 3)), (24, (1, 2)), (32, (1, 2)))
             for b in bs for z in (1, 3)]
 # x-pairs in 32-wide rows, two rows per warp (FP32)
-CONFIGS += [(b, r, z, "tiled_w32p") for r, bs in ((32, (1, 2, 3)), (48, (1, 2)))
+CONFIGS += [(b, r, z, "tiled_w32p") for r, bs in ((24, (1, 2)), (32, (1, 2, 3)), (48, (1, 2)))
             for b in bs for z in (1, 3)]
 # register-capped x-pair variants (2 CTAs of 16 rows / 4 CTAs of 8 rows per SM)
 CONFIGS += [(2, 16, 1, "tiled_w64:2"), (2, 16, 3, "tiled_w64:2"), (2, 8, 1, "tiled_w64:4"),

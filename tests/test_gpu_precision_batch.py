@@ -102,7 +102,7 @@ def test_16bit_storage_matches_rounded_oracle(storage, blt, rows):
 
 
 @pytest.mark.parametrize("storage", ["f16", "bf16", "f16e"])
-@pytest.mark.parametrize("blt,rows", [(1, 48), (2, 32), (2, 48), (3, 32)])
+@pytest.mark.parametrize("blt,rows", [(1, 24), (1, 48), (2, 24), (2, 32), (2, 48), (3, 32)])
 def test_16bit_pairs32_matches_rounded_oracle(storage, blt, rows):
     """The x-pair kernel with 32-cell rows (two per warp) and 16-bit storage."""
     shape, T = (70, 41, 33), 14

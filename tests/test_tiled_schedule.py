@@ -25,8 +25,8 @@ def bits_equal(a, b):
                           np.asarray(b, np.float32).view(np.uint32))
 
 
-CONFIGS = [(b, r, z, 32) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)), (32, (1, 2, 3, 4, 6)),
-                                       (48, (1, 2)))
+CONFIGS = [(b, r, z, 32) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)), (24, (1, 2)),
+                                       (32, (1, 2, 3, 4, 6)), (48, (1, 2)))
            for b in bs for z in (1, 3)]
 CONFIGS += [(b, r, z, 64) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4)), (20, (1, 2, 3)),
                                         (24, (1, 2)), (32, (1, 2)))
