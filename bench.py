@@ -122,8 +122,9 @@ def traffic_from_profile(cfg):
             continue
         kv = dict(part.split("=", 1) for part in ln.split() if "=" in part)
         try:
-            if (int(kv["blt"]), int(kv["tile_rows"]), int(kv["z_chunks"])) == \
-                    (cfg["blt"], cfg["tile_rows"], cfg["z_chunks"]):
+            if (kv["kernel"] == "fdtd_tiled2") == bool(cfg.get("pairs")) and \
+                    (int(kv["width"]), int(kv["blt"]), int(kv["tile_rows"]), int(kv["z_chunks"])) == \
+                    (cfg["width"], cfg["blt"], cfg["tile_rows"], cfg["z_chunks"]):
                 return float(kv["dram_bytes_per_launch"])
         except (KeyError, ValueError):
             continue
