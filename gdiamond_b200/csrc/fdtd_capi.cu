@@ -92,7 +92,7 @@ struct fdtd_handle {
   bool cfg_ready = false;
   CUtensorMap maps[2][6];
   CUtensorMap mat_map;
-  int maps_key = 0;  // width * 1000 + rows of the encoded boxes
+  int maps_key = 0;  // (field box width * 1000 + id box width) * 1000 + rows of the encoded boxes
   int last_kernel = 0, last_launches = 0;
   int last_folds = 0;  // DFT fold launches of the last fdtd_step
   int storage = FDTD_STORE_F32;
@@ -170,10 +170,16 @@ fdtd_status encode_map(fdtd_handle* h, CUtensorMap* m, void* base, CUtensorMapDa
   return FDTD_OK;
 }
 
-// Tensor maps of both field sets and of the material map for boxes {width, rows, 1} (fields)
-// and {width + 8, rows, 1} (material ids, widened so the box starts on an 8-element boundary).
-fdtd_status ensure_maps(fdtd_handle* h, int width, int rows) {
-  const int key = width * 1000 + rows;
+// Tensor maps of both field sets and of the material map for the boxes of kernel configuration
+// c: {row width + 8, rows, 1} for fields and ids of the x-pair family (boxes start at the tile
+// start rounded down to 8 elements); {32, rows, 1} for fields and {40, rows, 1} for ids of the
+// one-cell 32-wide kernel (its tile starts are 16-byte aligned).
+fdtd_status ensure_maps(fdtd_handle* h, const fdtd::TiledConfig& c) {
+  const bool pairs = c.width == 64 || c.pairs32;
+  const int width = pairs ? c.width + fdtd::kTiled2BoxPad : c.width;
+  const int mat_box = pairs ? c.width + fdtd::kTiled2BoxPad : fdtd::kMatBoxX;
+  const int rows = c.rows;
+  const int key = (width * 1000 + mat_box) * 1000 + rows;
   if (h->maps_key == key) return FDTD_OK;
   for (int s = 0; s < 2; ++s)
     for (int c = 0; c < 6; ++c) {
@@ -184,7 +190,6 @@ fdtd_status ensure_maps(fdtd_handle* h, int width, int rows) {
       fdtd_status st = encode_map(h, &h->maps[s][c], h->F[s][c], dt, comp_esz(h, c), width, rows);
       if (st != FDTD_OK) return st;
     }
-  const int mat_box = width == 64 ? fdtd::kMatBoxX2 : fdtd::kMatBoxX;
   fdtd_status st = encode_map(h, &h->mat_map, h->mat, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2,
                               mat_box, rows);
   if (st != FDTD_OK) return st;
@@ -344,7 +349,7 @@ fdtd_status autotune(fdtd_handle* h, cudaStream_t st) {
   CUDA_TRY(h, cudaEventCreate(&e1));
   // Time one candidate: one untimed launch, then `reps` timed launches; ms per step.
   auto time_cfg = [&](const fdtd::TiledConfig& c, int reps, float* per_step) -> fdtd_status {
-    fdtd_status s = ensure_maps(h, c.width, c.rows);
+    fdtd_status s = ensure_maps(h, c);
     if (s != FDTD_OK) return s;
     const fdtd::TiledArgs a = make_tiled_args(h, c, 0, false);
     CUDA_TRY(h, launch_any(c, a, h->g, st));
@@ -803,7 +808,7 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
     fdtd::TiledConfig c = h->cfg;
     c.storage = h->storage;  // the kernel instance must match this handle's field storage
     c.esz = h->esz;
-    s = ensure_maps(h, c.width, c.rows);
+    s = ensure_maps(h, c);
     if (s != FDTD_OK) return s;
     // The tiled kernels stage monitor-plane values in a ring of kDftSlots steps; a fold adds
     // them to the sums before the ring would wrap and once more at the end, so the sums are
@@ -1156,7 +1161,7 @@ fdtd_status batch_items(fdtd_batch* b, const fdtd::TiledConfig& c, std::pair<int
 
 fdtd_status batch_maps(fdtd_batch* b, const fdtd::TiledConfig& c) {
   for (fdtd_handle* h : b->sims) {
-    fdtd_status s = ensure_maps(h, c.width, c.rows);
+    fdtd_status s = ensure_maps(h, c);
     if (s != FDTD_OK) return bfail(b, s, "sim: %s", h->err.c_str());
   }
   return FDTD_OK;

@@ -73,20 +73,16 @@ __host__ __device__ constexpr int tiled_sy(int blt, int rows) { return rows - 2 
 constexpr int kTiledStages = 3;
 constexpr int kMatBoxX = 40;  // material box is widened to start on an 8-element boundary
 
-// Two-cells-per-thread family (k_tiled2.cu): 64-wide warp rows.  x tile starts are multiples
-// of 16 bytes of the stored type: al = 16 / esz elements.
-__host__ __device__ constexpr int tiled2_align(int esz) { return 16 / esz; }
-__host__ __device__ constexpr int tiled2_sx(int blt, int esz) {
-  return tiled2_align(esz) * ((64 - 2 * blt) / tiled2_align(esz));
-}
-__host__ __device__ constexpr int tiled2_sx_w(int w, int blt, int esz) {
-  return tiled2_align(esz) * ((w - 2 * blt) / tiled2_align(esz));
-}
-__host__ __device__ constexpr int tiled2_xbase(int blt, int esz) {
-  return -tiled2_align(esz) * ((blt + tiled2_align(esz) - 1) / tiled2_align(esz));
-}
+// Two-cells-per-thread family (k_tiled2.cu), w = 64 or 32 cells per warp row.  Tile x starts
+// need no TMA alignment: every box (fields and material ids) starts at the tile start rounded
+// down to 8 elements (16 bytes of any stored type) and is kTiled2BoxPad elements wider than the
+// row, so a tile writes all w - 2*blt columns of its last level whatever the storage type.  Tile
+// starts stay even so that the x-pairs' vector loads and stores stay aligned.
+constexpr int kTiled2BoxPad = 8;
+__host__ __device__ constexpr int tiled2_sx_w(int w, int blt) { return w - 2 * blt; }
+__host__ __device__ constexpr int tiled2_xbase(int blt) { return -2 * ((blt + 1) / 2); }
 constexpr int kTiled2Stages = 2;  // FP32; 16-bit storage uses one more
-constexpr int kMatBoxX2 = 72;     // 64 + 4 alignment offset, rounded to a 16-byte row
+constexpr int kMatBoxX2 = 64 + kTiled2BoxPad;  // box width of 64-cell rows (fields and ids)
 bool tiled2_config_supported(const TiledConfig& c);
 dim3 tiled2_grid(const TiledConfig& c, const Grid& g);
 cudaError_t launch_tiled2(const TiledConfig& c, const TiledArgs& args, const Grid& g,

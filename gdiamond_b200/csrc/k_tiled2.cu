@@ -20,8 +20,9 @@
 // storage no scaling is applied and every multiply/add is separately rounded: results are
 // bit-identical to the reference CPU update.
 //
-// x tile starts are multiples of 16 bytes of the narrower stored type (4 floats, 8 halves): the
-// TMA rule for the innermost coordinate, for both types.
+// x tile starts are even but otherwise free: the TMA boxes start at the tile start rounded down
+// to 8 elements (16 bytes of either stored type: the TMA rule for the innermost coordinate) and
+// are 8 elements wider than the row; threads index the staged planes from the remainder.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -85,26 +86,30 @@ template <typename S, int B, int TY, int W = 64, typename SH = S>
 struct Tiled2 {
   static constexpr int ESZ_E = (int)sizeof(S);    // stored E value
   static constexpr int ESZ_H = (int)sizeof(SH);   // stored H value
-  static constexpr int ESZ = ESZ_E < ESZ_H ? ESZ_E : ESZ_H;  // x alignment unit
+  static constexpr int ESZ = ESZ_E < ESZ_H ? ESZ_E : ESZ_H;
   static constexpr int LPR = W / 2;            // lanes per tile row
   static constexpr int THREADS = TY * LPR;
-  static constexpr int MBX = W == 64 ? kMatBoxX2 : kMatBoxX;  // material box width
-  static constexpr int PL = W * TY;            // elements of one staged field plane
+  static constexpr int WB = W + kTiled2BoxPad;  // box width of fields and material ids
+  static constexpr int MBX = WB;
+  static constexpr int PL = WB * TY;           // elements of one staged field plane
+  static constexpr int PLX = W * TY;           // elements of one y-exchange plane
   static constexpr int MPL = MBX * TY;         // elements of one staged material plane
   static constexpr int MPL_S = (MPL * 2 + 127) / 128 * 64;  // its stage stride: 128-byte steps
   static constexpr int NS = ESZ_E + ESZ_H == 8 ? kTiled2Stages : kTiled2Stages + 1;
-  static constexpr int SX = tiled2_sx_w(W, B, ESZ);
+  static constexpr int SX = tiled2_sx_w(W, B);
   static constexpr int SY = tiled_sy(B, TY);
-  static constexpr int XBASE = tiled2_xbase(B, ESZ);
+  static constexpr int XBASE = tiled2_xbase(B);
   static constexpr uint32_t OFF_HPLANES = 3u * PL * ESZ_E;  // H planes follow E in a stage
   static constexpr uint32_t STAGE_F_BYTES = 3u * PL * (ESZ_E + ESZ_H);
   static constexpr uint32_t STAGE_M_BYTES = MPL_S * 2u;  // TMA destinations stay 128-aligned
   static constexpr uint32_t TX_BYTES = STAGE_F_BYTES + MPL * 2u;  // bytes the copies deliver
   static constexpr size_t OFF_M = (size_t)NS * STAGE_F_BYTES;
   static constexpr size_t OFF_H = OFF_M + (size_t)NS * STAGE_M_BYTES;
-  static constexpr size_t OFF_E = OFF_H + 2u * 2u * PL * 4u;
-  static constexpr size_t OFF_BAR = OFF_E + (size_t)B * 2u * PL * 4u;
+  static constexpr size_t OFF_E = OFF_H + 2u * 2u * PLX * 4u;
+  static constexpr size_t OFF_BAR = OFF_E + (size_t)B * 2u * PLX * 4u;
   static constexpr size_t SMEM = OFF_BAR + NS * 8u + 128u;  // + alignment slack
+  static_assert(SMEM <= 227u * 1024u, "shared memory per CTA");
+  static_assert(SX % 2 == 0 && XBASE % 2 == 0 && XBASE + B <= 0, "even tile starts");
   static_assert(SY >= 1, "tile too short for this BLT");
   static_assert((W == 64 || W == 32) && THREADS % 32 == 0, "warp rows of 64 or 32 cells");
   static_assert(STAGE_M_BYTES % 128 == 0 && (PL * ESZ) % 128 == 0, "stage alignment");
@@ -141,8 +146,8 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   using StH = Store<SH>;  // H components
   unsigned char* st_f = sm.base;  // per stage: Ex Ey Ez as S, then Hx Hy Hz as SH
   uint16_t* st_m = reinterpret_cast<uint16_t*>(sm.base + K::OFF_M);
-  float* hbuf = reinterpret_cast<float*>(sm.base + K::OFF_H);  // [2][Hz,Hx][PL]
-  float* ebuf = reinterpret_cast<float*>(sm.base + K::OFF_E);  // [B][Ex,Ez][PL]
+  float* hbuf = reinterpret_cast<float*>(sm.base + K::OFF_H);  // [2][Hz,Hx][PLX]
+  float* ebuf = reinterpret_cast<float*>(sm.base + K::OFF_E);  // [B][Ex,Ez][PLX]
   uint64_t* bars = sm.bars;
 
   const Grid g = a.g;
@@ -155,7 +160,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   const int lx = threadIdx.x % K::LPR;                                   // pair in the row
   const int ly = threadIdx.y * (32 / K::LPR) + threadIdx.x / K::LPR;     // tile row
   const int tid = threadIdx.y * 32 + threadIdx.x;
-  const int X = bx * K::SX + K::XBASE;  // multiple of 16 bytes of S and of SH
+  const int X = bx * K::SX + K::XBASE;  // even; the boxes start at X8
   const int Y = by * K::SY - B;
   const int X8 = X & ~7;
   const int cx0 = 2 * lx;               // tile column of the even cell
@@ -195,7 +200,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     inv[c] = scaled ? a.inv_scale[c] : 1.0f;
   }
 
-  for (int q = tid; q < (4 + 2 * B) * K::PL; q += K::THREADS) hbuf[q] = 0.0f;
+  for (int q = tid; q < (4 + 2 * B) * K::PLX; q += K::THREADS) hbuf[q] = 0.0f;
   __syncthreads();  // zeroed exchange planes; the previous tile's stages are all consumed
 
   auto issue = [&](int it_) {
@@ -209,8 +214,8 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     const int pz = ps + it_;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      tma_load_3d(de + c * K::PL, &a.tm_src[c], bar, X, Y, pz);
-      tma_load_3d(dh + c * K::PL, &a.tm_src[3 + c], bar, X, Y, pz);
+      tma_load_3d(de + c * K::PL, &a.tm_src[c], bar, X8, Y, pz);
+      tma_load_3d(dh + c * K::PL, &a.tm_src[3 + c], bar, X8, Y, pz);
     }
     tma_load_3d(st_m + stage * K::MPL_S, &a.tm_mat, bar, X8, Y, pz);
   };
@@ -229,10 +234,14 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
 #pragma unroll
   for (int s = 0; s <= B; ++s) mq[s] = 0;
 
+  // y-exchange planes: W per row; staged planes (fields and ids): WB per row from X8
   const int o = ly * W + cx0;
   const int oym = (ly > 0 ? ly - 1 : 0) * W + cx0;
   const int oyp = (ly < TY - 1 ? ly + 1 : TY - 1) * W + cx0;
-  const int om = ly * K::MBX + cx0 + (X - X8);  // even: a 4-byte aligned id pair
+  const int xoff = X - X8;                   // even, 0..6
+  const int os = ly * K::WB + cx0 + xoff;    // even: aligned pair loads
+  const int osym = (ly > 0 ? ly - 1 : 0) * K::WB + cx0 + xoff;
+  const int om = ly * K::MBX + cx0 + xoff;   // even: a 4-byte aligned id pair
   const float dx = a.dx;
   const long long pitch = g.pitch, plane = g.plane;
   S* const* dst = reinterpret_cast<S* const*>(a.dst.f);        // E components
@@ -260,13 +269,13 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     Pair Hc[3], Eo[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float2 hv = StH::ld2(H0 + c * K::PL + o, sc[3 + c]);
-      const float2 ev = St::ld2(E0 + c * K::PL + o, sc[c]);
+      const float2 hv = StH::ld2(H0 + c * K::PL + os, sc[3 + c]);
+      const float2 ev = St::ld2(E0 + c * K::PL + os, sc[c]);
       Hc[c] = Pair{hv.x, hv.y};
       Eo[c] = Pair{ev.x, ev.y};
     }
-    float2 hz_ym = StH::ld2(H0 + 2 * K::PL + oym, sc[5]);
-    float2 hx_ym = StH::ld2(H0 + oym, sc[3]);
+    float2 hz_ym = StH::ld2(H0 + 2 * K::PL + osym, sc[5]);
+    float2 hx_ym = StH::ld2(H0 + osym, sc[3]);
     Pair EnPrev[3] = {};
     Pair EnB[3] = {}, HnB[3] = {};
 
@@ -315,8 +324,8 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
       // x+1 neighbour: own odd cell for the even cell, even cell of lane+1 for the odd cell
       const float ez_xp = __shfl_down_sync(kFull, Ep[s][2].a, 1, K::LPR);
       const float ey_xp = __shfl_down_sync(kFull, Ep[s][1].a, 1, K::LPR);
-      float* eb = ebuf + (s - 1) * 2 * K::PL;
-      const float2 ex_yp = ldf2(eb + oyp), ez_yp = ldf2(eb + K::PL + oyp);
+      float* eb = ebuf + (s - 1) * 2 * K::PLX;
+      const float2 ex_yp = ldf2(eb + oyp), ez_yp = ldf2(eb + K::PLX + oyp);
       cxp.a = sub(sub(En[1].a, Ep[s][1].a), sub(ez_yp.x, Ep[s][2].a));
       cxp.b = sub(sub(En[1].b, Ep[s][1].b), sub(ez_yp.y, Ep[s][2].b));
       cyp.a = sub(sub(Ep[s][2].b, Ep[s][2].a), sub(En[0].a, Ep[s][0].a));
@@ -365,13 +374,13 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
       }
       // ---------------- exchange
       if (s < B) {
-        float* hb = hbuf + (s & 1) * 2 * K::PL;
+        float* hb = hbuf + (s & 1) * 2 * K::PLX;
         stf2(hb + o, Hn[2].a, Hn[2].b);
-        stf2(hb + K::PL + o, Hn[0].a, Hn[0].b);
+        stf2(hb + K::PLX + o, Hn[0].a, Hn[0].b);
       }
       __syncthreads();
       stf2(eb + o, En[0].a, En[0].b);
-      stf2(eb + K::PL + o, En[2].a, En[2].b);
+      stf2(eb + K::PLX + o, En[2].a, En[2].b);
       if (s == 1) {
         abort = *sm.abort != 0;
         if (!abort && tid == 0 && it + K::NS < niter) {
@@ -390,9 +399,9 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
         Hp[s - 1][c] = Hc[c];
       }
       if (s < B) {
-        const float* hb = hbuf + (s & 1) * 2 * K::PL;
+        const float* hb = hbuf + (s & 1) * 2 * K::PLX;
         hz_ym = ldf2(hb + oym);
-        hx_ym = ldf2(hb + K::PL + oym);
+        hx_ym = ldf2(hb + K::PLX + oym);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           Hc[c] = Hn[c];
@@ -765,8 +774,8 @@ bool tiled2_batch_supported(const TiledConfig& c) {
 }
 
 dim3 tiled2_grid(const TiledConfig& c, const Grid& g) {
-  const int sx = tiled2_sx_w(c.pairs32 ? 32 : 64, c.blt, c.esz), sy = tiled_sy(c.blt, c.rows);
-  const int first = tiled2_xbase(c.blt, c.esz) + c.blt;
+  const int sx = tiled2_sx_w(c.pairs32 ? 32 : 64, c.blt), sy = tiled_sy(c.blt, c.rows);
+  const int first = tiled2_xbase(c.blt) + c.blt;
   const int ntx = (g.nx - first + sx - 1) / sx;
   const int nty = (g.ny + sy - 1) / sy;
   const int zlen = (g.nz + c.z_chunks - 1) / c.z_chunks;

@@ -25,16 +25,20 @@ def bits_equal(a, b):
                           np.asarray(b, np.float32).view(np.uint32))
 
 
-CONFIGS = [(b, r, z, 32) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)), (24, (1, 2)),
-                                       (32, (1, 2, 3, 4, 6)), (48, (1, 2)))
+# (blt, rows, z-chunks, row width, x-pair family): the one-cell kernel (32-cell rows) and the
+# x-pair kernel's 64- and 32-cell rows, at every instance the library builds
+CONFIGS = [(b, r, z, 32, False) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4, 5, 6)),
+                                              (32, (1, 2, 3, 4, 6)))
            for b in bs for z in (1, 3)]
-CONFIGS += [(b, r, z, 64) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4)), (20, (1, 2, 3)),
-                                        (24, (1, 2)), (32, (1, 2)))
+CONFIGS += [(b, r, z, 64, True) for r, bs in ((8, (1, 2, 3)), (16, (1, 2, 3, 4)), (20, (1, 2, 3)),
+                                              (24, (1, 2)), (32, (1, 2)))
+            for b in bs for z in (1, 3)]
+CONFIGS += [(b, r, z, 32, True) for r, bs in ((24, (1, 2)), (32, (1, 2, 3)), (48, (1, 2)))
             for b in bs for z in (1, 3)]
 
 
-@pytest.mark.parametrize("blt,rows,zc,width", CONFIGS)
-def test_schedule_point_sources(blt, rows, zc, width):
+@pytest.mark.parametrize("blt,rows,zc,width,pairs", CONFIGS)
+def test_schedule_point_sources(blt, rows, zc, width, pairs):
     shape, T = (71 if width == 64 else 37, 21, 19), 7
     coefs = oracle.coefficients(shape)
     w = wave(T)
@@ -42,14 +46,17 @@ def test_schedule_point_sources(blt, rows, zc, width):
         oracle.Source("Jz", w, i=18, j=10, k=9), oracle.Source("Mx", w * np.float32(0.5), i=5, j=6, k=7)])
     F = TE.run(shape, coefs, T, blt, rows, zc, DX, sources=[
         dict(comp=2, kind=0, i=18, j=10, k=9, wave=w),
-        dict(comp=3, kind=0, i=5, j=6, k=7, wave=w * np.float32(0.5))], width=width)
+        dict(comp=3, kind=0, i=5, j=6, k=7, wave=w * np.float32(0.5))], width=width,
+        pairs=pairs)
     for c in range(6):
         assert bits_equal(F[c], F_ref[c]), oracle.COMPONENTS[c]
 
 
-@pytest.mark.parametrize("blt,rows,zc,width", [(2, 8, 2, 32), (4, 16, 3, 32), (3, 16, 1, 32),
-                                               (6, 32, 2, 32), (3, 16, 2, 64), (2, 32, 1, 64)])
-def test_schedule_plane_source_and_monitors(blt, rows, zc, width):
+@pytest.mark.parametrize("blt,rows,zc,width,pairs",
+                         [(2, 8, 2, 32, False), (4, 16, 3, 32, False), (3, 16, 1, 32, False),
+                          (6, 32, 2, 32, False), (3, 16, 2, 64, True), (2, 32, 1, 64, True),
+                          (1, 24, 2, 32, True), (3, 32, 1, 32, True)])
+def test_schedule_plane_source_and_monitors(blt, rows, zc, width, pairs):
     shape, T = (29, 23, 17), 9
     nx, ny, nz = shape
     rng = np.random.default_rng(1)
@@ -68,7 +75,7 @@ def test_schedule_plane_source_and_monitors(blt, rows, zc, width):
                   im=np.zeros((3, ny, nx)))]
     F = TE.run(shape, coefs, T, blt, rows, zc, DX,
                sources=[dict(comp=2, kind=1, i=0, j=0, k=4, wave=w)], monitors=emons,
-               width=width)
+               width=width, pairs=pairs)
     for c in range(6):
         assert bits_equal(F[c], F_ref[c]), oracle.COMPONENTS[c]
     for em, om in zip(emons, mons):
@@ -78,16 +85,17 @@ def test_schedule_plane_source_and_monitors(blt, rows, zc, width):
 
 def test_output_windows_tile_the_grid():
     """Every cell is written exactly once per pass and nothing outside the grid."""
-    for width, blt, rows in [(w, b, r) for w in (32, 64) for b in range(1, 7)
-                             for r in (8, 16, 20, 24, 32, 48)]:
+    for (width, pairs), blt, rows in [(wp, b, r) for wp in ((32, False), (32, True), (64, True))
+                                      for b in range(1, 7) for r in (8, 16, 20, 24, 32, 48)]:
         if rows - 2 * blt < 1:
             continue
         for shape in ((3, 3, 3), (33, 17, 9), (100, 61, 5)):
             nx, ny, nz = shape
-            sx, xbase, sy = TE.tile_geometry(blt, rows, width)
-            assert sx % 4 == 0 and xbase % 4 == 0 and xbase + blt <= 0
+            sx, xbase, sy = TE.tile_geometry(blt, rows, width, pairs)
+            align = 2 if pairs else 4  # x-pairs: even starts; one cell: 16-byte TMA starts
+            assert sx % align == 0 and xbase % align == 0 and xbase + blt <= 0
             assert sx <= width - 2 * blt
-            ntx, nty, nzc, zlen = TE.grid_dims(shape, blt, rows, 2, width)
+            ntx, nty, nzc, zlen = TE.grid_dims(shape, blt, rows, 2, width, pairs)
             cover = np.zeros(nx, int)
             for bx in range(ntx):
                 lo = bx * sx + xbase + blt

@@ -16,16 +16,26 @@ from __future__ import annotations
 import numpy as np
 
 
-def tile_geometry(blt, rows, width=32):
-    sx = 4 * ((width - 2 * blt) // 4)
-    xbase = -4 * ((blt + 3) // 4)
+def tile_geometry(blt, rows, width=32, pairs=None):
+    """(sx, xbase, sy).  One-cell kernel (fdtd_tiled): x tile starts are multiples of 4 floats
+    (the TMA rule).  x-pair family (fdtd_tiled2, 64- or 32-cell rows; pairs defaults to
+    width == 64): the boxes start at the tile start rounded down to 8 elements, so tile starts
+    only need to be even and a tile writes width - 2*blt columns."""
+    if pairs is None:
+        pairs = width == 64
+    if pairs:
+        sx = width - 2 * blt
+        xbase = -2 * ((blt + 1) // 2)
+    else:
+        sx = 4 * ((width - 2 * blt) // 4)
+        xbase = -4 * ((blt + 3) // 4)
     sy = rows - 2 * blt
     return sx, xbase, sy
 
 
-def grid_dims(shape, blt, rows, z_chunks, width=32):
+def grid_dims(shape, blt, rows, z_chunks, width=32, pairs=None):
     nx, ny, nz = shape
-    sx, xbase, sy = tile_geometry(blt, rows, width)
+    sx, xbase, sy = tile_geometry(blt, rows, width, pairs)
     first = xbase + blt
     ntx = -(-(nx - first) // sx)
     nty = -(-ny // sy)
@@ -92,13 +102,14 @@ def _source_value(sources, comp, x, y, e, t, dx):
 
 
 def tiled_pass(shape, F, mat, table, blt, rows, z_chunks, t0, dx, sources=(), monitors=(),
-               width=32):
+               width=32, pairs=None):
     """One launch: BLT steps from field set F (6 flat float32 arrays) into a new set.
-    width 32 emulates fdtd_tiled (k_tiled.cu), width 64 fdtd_tiled2 (k_tiled2.cu)."""
+    width 32 emulates fdtd_tiled (k_tiled.cu) or, with pairs, fdtd_tiled2's 32-cell rows;
+    width 64 emulates fdtd_tiled2's 64-cell rows (k_tiled2.cu)."""
     nx, ny, nz = shape
     B, TY, W = blt, rows, width
-    sx, xbase, sy = tile_geometry(B, TY, W)
-    ntx, nty, nzc, zlen = grid_dims(shape, B, TY, z_chunks, W)
+    sx, xbase, sy = tile_geometry(B, TY, W, pairs)
+    ntx, nty, nzc, zlen = grid_dims(shape, B, TY, z_chunks, W, pairs)
     F3 = [np.asarray(f, np.float32).reshape(nz, ny, nx) for f in F]
     M3 = mat.reshape(nz, ny, nx)
     dst = [np.full((nz, ny, nx), np.nan, np.float32) for _ in range(6)]
@@ -210,7 +221,7 @@ def tiled_pass(shape, F, mat, table, blt, rows, z_chunks, t0, dx, sources=(), mo
 
 
 def run(shape, coefs, T, blt, rows, z_chunks, dx, sources=(), monitors=(), fields=None,
-        width=32):
+        width=32, pairs=None):
     """T steps in passes of BLT (a final shorter pass for the remainder), as fdtd_step."""
     nx, ny, nz = shape
     mat, table = material_table(coefs)
@@ -218,6 +229,7 @@ def run(shape, coefs, T, blt, rows, z_chunks, dx, sources=(), monitors=(), field
     t = 0
     while t < T:
         b = min(blt, T - t)
-        F = tiled_pass(shape, F, mat, table, b, rows, z_chunks, t, dx, sources, monitors, width)
+        F = tiled_pass(shape, F, mat, table, b, rows, z_chunks, t, dx, sources, monitors, width,
+                       pairs)
         t += b
     return F
