@@ -352,11 +352,20 @@ def run_ours(args):
 # ------------------------------------------------------------------ other configurations
 
 
+def _rel(num, den):
+    """sqrt(num / den); a zero reference (a monitor the pulse has not reached) counts as exact
+    when the result is zero too, and as an infinite error otherwise."""
+    num, den = float(num), float(den)
+    if den == 0.0:
+        return 0.0 if num == 0.0 else float("inf")
+    return float(np.sqrt(num / den))
+
+
 def _spectral_error(a, b):
     """Relative L2 error of complex spectra a = (re, im) lists against b."""
     num = sum(np.sum((ar - br) ** 2 + (ai - bi) ** 2) for (ar, ai), (br, bi) in zip(a, b))
     den = sum(np.sum(br ** 2 + bi ** 2) for (br, bi) in b)
-    return float(np.sqrt(num / den))
+    return _rel(num, den)
 
 
 def _plane_spectrum_error(a, b):
@@ -368,7 +377,7 @@ def _plane_spectrum_error(a, b):
         sb = br.sum(axis=(1, 2)) + 1j * bi.sum(axis=(1, 2))
         num += float(np.sum(np.abs(sa - sb) ** 2))
         den += float(np.sum(np.abs(sb) ** 2))
-    return float(np.sqrt(num / den))
+    return _rel(num, den)
 
 
 def _field_error(F, R):
