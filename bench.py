@@ -185,6 +185,85 @@ def run_reference_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------ reference GPU paths
+
+
+REF_GPU_RUNS = (
+    # (binary, driver arguments Tx Ty Tz T, grid, steps): the legal sizes nearest 256^3
+    ("gpu_mm_ver2", ("9", "23", "23", "999"), (268, 262, 262), 999),
+    ("gpu_mm_ver3", ("20", "52", "52", "1000"), (260, 260, 260), 1000),
+)
+
+
+def _parse_reference_output(text):
+    """(label, seconds, Mcells/s) of every timed path in a reference example's stdout: lines
+    'gpu runtime (<label>): <s>s' each followed by 'gpu performance: <x>Mcells/s'."""
+    import re
+    out, label, secs = [], None, None
+    for ln in text.splitlines():
+        m = re.match(r"gpu runtime \((.*)\): ([0-9.eE+-]+)s", ln.strip())
+        if m:
+            label, secs = m.group(1), float(m.group(2))
+            continue
+        m = re.match(r"gpu performance: ([0-9.eE+-]+)\s*Mcells/s", ln.strip())
+        if m and label is not None:
+            out.append((label, secs, float(m.group(1))))
+            label = None
+    return out
+
+
+def reference_gpu_results(timeout=300):
+    """The reference's own GPU paths on this GPU: examples/gpu_mm_ver2.cu and gpu_mm_ver3.cu
+    compiled unmodified for sm_100a (oracle/_ref, built from the reference sources by
+    oracle/Makefile).  Each runs the naive path (update_FDTD_gpu_3D_warp_underutilization_fix)
+    and its mix-mapping path at a legal grid size and times them with its own host clock around
+    the launch loop (synchronised); the driver then checks the two against each other.  Our
+    solver runs the same grid and step count (the reference constructor's coefficients, a
+    Gaussian Jz point source at the centre), timed with CUDA events after its autotuning."""
+    import torch
+    import gdiamond_b200 as gd
+    from gdiamond_b200 import workloads as W
+    res = {}
+    for binary, argv, shape, T in REF_GPU_RUNS:
+        path = os.path.join(ROOT, "oracle", "_ref", binary)
+        key = f"{binary}_{shape[0]}x{shape[1]}x{shape[2]}_T{T}"
+        if not os.path.exists(path):
+            res[key] = {"unavailable": f"{path} not built"}
+            continue
+        try:
+            r = subprocess.run([path, *argv], capture_output=True, text=True, timeout=timeout)
+            runs = _parse_reference_output(r.stdout)
+            entry = {"returncode": r.returncode,
+                     "checked_by_driver": "results are matched" in r.stderr,
+                     "paths": {lab: {"seconds": sec, "gcells": mc / 1e3} for lab, sec, mc in runs}}
+        except subprocess.TimeoutExpired:
+            entry = {"unavailable": f"timed out after {timeout} s"}
+        # ours, same grid and steps
+        nx, ny, nz = shape
+        sim = gd.Simulation(nx, ny, nz)
+        sim.set_coefficients(W.reference_coefficients(shape))
+        sim.set_sources([dict(component="Jz", wave=W.gaussian_wave(T), i=nx // 2, j=ny // 2,
+                              k=nz // 2)])
+        sim.step(8)  # autotune and warm-up
+        sim.reset()
+        st = torch.cuda.Stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        sim.step(T, stream=st)
+        e1.record(st)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        cfg = sim.config()
+        sim.close()
+        entry["ours"] = {"seconds": sec, "gcells": nx * ny * nz * T / sec / 1e9,
+                         "kernel": cfg}
+        for lab, v in entry.get("paths", {}).items():
+            entry["ours"][f"speedup_vs_{lab.replace(' ', '_')}"] = v["seconds"] / sec
+        res[key] = entry
+    return res
+
+
 # ------------------------------------------------------------------ our arm
 
 
@@ -225,6 +304,7 @@ def run_ours(args):
     sim = gd.Simulation(nx, ny, nz, device=local, kernel=args.kernel, blt=args.blt,
                         tile_rows=args.rows, z_chunks=args.zchunks, min_blocks=args.min_blocks)
     sim.set_coefficients(coefs)
+    sim.set_fast_path(not args.no_fast_path)
     sim.set_sources(src)
     mid = sim.add_dft_monitor("Ez", nz // 2, freqs, scale=1.0)
     stream = torch.cuda.Stream()
@@ -239,6 +319,7 @@ def run_ours(args):
     stream.synchronize()
     sim.sync()
     cfg = sim.config()
+    sim_fast = sim.fast_path
     launches_per_step = cfg["launches"]
 
     # ---------------- device-resident timed region
@@ -319,6 +400,19 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    extra = None
+    if world == 1 and not args.no_extras and (shape, T_run) == (SHAPE, T_STEPS):
+        extra = {}
+        for name, fn in (("mixed", lambda: mixed_results(args)),
+                         ("batched", lambda: batched_results(args, ("f16e", "f32"),
+                                                             one_at_a_time=False)),
+                         ("reference_gpu", reference_gpu_results)):
+            try:
+                t0 = time.perf_counter()
+                extra[name] = fn()
+                extra[name]["wall_seconds"] = time.perf_counter() - t0
+            except Exception as e:  # an extra configuration must not void the main line
+                extra[name] = {"unavailable": f"{type(e).__name__}: {e}"}
     line = {
         "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -330,7 +424,7 @@ def run_ours(args):
                    "dft_freqs": N_FREQS, "kernel": cfg["kernel"], "width": cfg.get("width"),
                    "blt": cfg["blt"],
                    "tile_rows": cfg["tile_rows"], "z_chunks": cfg["z_chunks"],
-                   "min_blocks": cfg["min_blocks"],
+                   "min_blocks": cfg["min_blocks"], "fast_path": sim_fast,
                    "parallelism": f"replicas{world}",
                    "l2": "inputs (1.2 GB of fields) larger than L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -344,6 +438,7 @@ def run_ours(args):
         "e2e": e2e,
         "gpu_launches": (launches_per_step + cfg["dft_folds"]) * args.steps,
         "clocks": clk,
+        "extra": extra,
     }
     print(json.dumps(line))
     return 0
@@ -421,10 +516,16 @@ def fp16_scales(probe, ncell, T, every=1, headroom=2048.0):
 
 
 def run_mixed(args):
+    print(json.dumps(mixed_results(args)))
+    return 0
+
+
+def mixed_results(args, storages=("f32", "bf16", "f16", "f16e")):
     """Mixed-precision FDTD: 512x512x384 grid, 200 seeded dielectric spheres, Gaussian Jz at the
     centre, FP64 running DFT of Ez at 16 frequencies on the planes z=96 and z=288, 2000 steps.
     FP32, BF16, FP16 and F16E (FP16 E, FP32 H) field storage against an FP64 run of the same
-    grid."""
+    grid.  FP16 scales come from an FP32 probe of the first 400 steps; its time is reported and
+    included in the `gcells_incl_scale_probe` rates."""
     import torch
     import gdiamond_b200 as gd
     from gdiamond_b200 import workloads as W
@@ -456,9 +557,12 @@ def run_mixed(args):
     nmat = ref.material_count()
     ref.close()
     res["f64"] = {"gcells": ncell * T / t64 / 1e9, "seconds": t64}
+    t0 = time.perf_counter()
     f16_scales = fp16_scales(make("f32"), ncell, min(T, 400))
-    for storage, scales in (("f32", None), ("bf16", None), ("f16", f16_scales),
-                            ("f16e", f16_scales)):
+    t_probe = time.perf_counter() - t0
+    t32 = None
+    for storage in storages:
+        scales = f16_scales if storage in ("f16", "f16e") else None
         sim = make(storage, scales)
         sim.step(2 * 4)  # autotune + warm-up outside the timed run
         sim.reset()
@@ -467,19 +571,29 @@ def run_mixed(args):
         D = [sim.get_dft(m) for m in range(2)]
         cfg = sim.config()
         sim.close()
+        if storage == "f32":
+            t32 = dt_
         res[storage] = {"gcells": ncell * T / dt_ / 1e9, "seconds": dt_,
                         "spectral_rel_err_vs_f64": _spectral_error(D, D64),
                         "plane_spectrum_rel_err_vs_f64": _plane_spectrum_error(D, D64),
                         "field_rel_l2_vs_f64": _field_error(F, R),
                         "kernel": cfg, "scales": scales}
-    line = {"metric": "Gcell-updates/s and relative error vs FP64", "workload":
+        if scales is not None:
+            res[storage]["gcells_incl_scale_probe"] = ncell * T / (dt_ + t_probe) / 1e9
+        if t32 is not None:
+            res[storage]["speedup_vs_f32"] = t32 / dt_
+    return {"metric": "Gcell-updates/s and relative error vs FP64", "workload":
             f"fdtd3d_{nx}x{ny}x{nz}_200spheres_gaussJz_T{T}_dft16x2planes",
-            "materials": nmat, "results": res, "data": "synthetic (seeded spheres)"}
-    print(json.dumps(line))
-    return 0
+            "materials": nmat, "fp16_scale_probe_seconds": t_probe, "results": res,
+            "data": "synthetic (seeded spheres)"}
 
 
 def run_batched(args):
+    print(json.dumps(batched_results(args, args.batch_storage.split(","))))
+    return 0
+
+
+def batched_results(args, storages, one_at_a_time=True):
     """64 independent uneven simulations (sides from {64,96,128,160,192} per axis, seeded), one
     dielectric slab each, Gaussian Jz at a random interior point, 32-frequency DFT of Ez on one
     plane each, 2000 steps.  Spectra/s of the batched persistent solver (16-bit storage,
@@ -531,7 +645,7 @@ def run_batched(args):
 
     t64, D64 = run_each("f64")
     t32, D32 = run_each("f32")
-    t32s, _ = run_each("f32", sync_each=True)
+    t32s, _ = run_each("f32", sync_each=True) if one_at_a_time else (t32, None)
     out = {"plain_f32_sim_by_sim": {"seconds": t32, "spectra_per_s": n_sims / t32,
                                     "gcells": total_cells * T / t32 / 1e9,
                                     "streams": "overlapped (one stream per handle)",
@@ -547,7 +661,7 @@ def run_batched(args):
     shape0, _, pos0 = specs[small]
     f16 = fp16_scales(make((shape0, np.ones(int(np.prod(shape0)), np.float32), pos0), "f32"),
                       int(np.prod(shape0)), min(T, 300))
-    for storage in args.batch_storage.split(","):
+    for storage in storages:
         scales = f16 if storage in ("f16", "f16e") else None  # f16e scales E only
         sims = [make(sp, storage, scales, blt=args.blt) for sp in specs]
         batch = gd.Batch(sims)
@@ -577,11 +691,9 @@ def run_batched(args):
             "spectral_rel_err_vs_f64_max": float(np.max(errs)),
             "plane_spectrum_rel_err_vs_f64_mean": float(np.mean(perrs)),
             "plane_spectrum_rel_err_vs_f64_max": float(np.max(perrs)), "config": cfg}
-    line = {"metric": "spectra/s (batched vs plain) at stated spectral error vs FP64",
+    return {"metric": "spectra/s (batched vs plain) at stated spectral error vs FP64",
             "workload": f"{n_sims} uneven sims, sides from {sides}, slab each, T={T}, 32-freq DFT",
             "total_cells": total_cells, "results": out, "data": "synthetic (seeded)"}
-    print(json.dumps(line))
-    return 0
 
 
 def run_surrogate(args):
@@ -748,6 +860,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer run")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-precision, batched and reference-GPU lines that the "
+                         "default run adds under 'extra'")
     ap.add_argument("--grid", default="256,256,256", help="NX,NY,NZ (profiling cases)")
     ap.add_argument("--timesteps", type=int, default=T_STEPS)
     ap.add_argument("--kernel", default="auto",
@@ -756,6 +871,8 @@ def main():
     ap.add_argument("--rows", type=int, default=0, help="force tile rows")
     ap.add_argument("--zchunks", type=int, default=0, help="force z-chunks")
     ap.add_argument("--min-blocks", type=int, default=0, help="force the register cap")
+    ap.add_argument("--no-fast-path", action="store_true",
+                    help="force the general per-cell path of the x-pair kernels")
     ap.add_argument("--workload", default="plain",
                     choices=["plain", "mixed", "batched", "surrogate", "mlp"],
                     help="plain: the benchmark line; mixed / batched: the precision and "

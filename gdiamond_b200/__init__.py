@@ -41,7 +41,8 @@ EXPORTS = (
     "fdtd_mlp_train", "fdtd_mlp_predict", "fdtd_mlp_predict_device", "fdtd_get_dft_device",
     "fdtd_mlp_set_gemm", "fdtd_get_planes_device", "fdtd_set_planes_device",
     "fdtd_storage_bytes", "fdtd_set_step", "fdtd_set_dft", "fdtd_component_bytes",
-    "fdtd_dft_folds",
+    "fdtd_dft_folds", "fdtd_set_fast_path", "fdtd_fast_path", "fdtd_add_flux_monitor",
+    "fdtd_get_flux", "fdtd_get_flux_device", "fdtd_flux_monitor_ids",
 )
 
 
@@ -103,6 +104,13 @@ def library():
             "fdtd_storage_bytes": ([V, P(C.c_int32)], C.c_int),
             "fdtd_component_bytes": ([V, C.c_int32, P(C.c_int32)], C.c_int),
             "fdtd_dft_folds": ([V, P(C.c_int32)], C.c_int),
+            "fdtd_set_fast_path": ([V, C.c_int32], C.c_int),
+            "fdtd_add_flux_monitor": ([V, C.c_int64, P(C.c_double), C.c_int32, C.c_double,
+                                       P(C.c_int32)], C.c_int),
+            "fdtd_get_flux": ([V, C.c_int32, P(C.c_double)], C.c_int),
+            "fdtd_get_flux_device": ([V, C.c_int32, V, V], C.c_int),
+            "fdtd_flux_monitor_ids": ([V, C.c_int32, P(C.c_int32)], C.c_int),
+            "fdtd_fast_path": ([V, P(C.c_int32)], C.c_int),
             "fdtd_set_step": ([V, C.c_int64], C.c_int),
             "fdtd_set_dft": ([V, C.c_int32, P(C.c_double), P(C.c_double)], C.c_int),
             "fdtd_batch_create": ([P(V), C.c_int32, P(V)], C.c_int),
@@ -168,9 +176,12 @@ class Simulation:
             raise FdtdError(st, self._L.fdtd_last_error(None).decode())
         self._h = h
         self._device = int(device)
+        self.storage = storage
+        self.storage_scale = [1.0] * 6  # value = stored * scale (16-bit components)
         self._keep = []
         self.n_monitors = 0
         self._monitor_nf = []
+        self._flux_nf = []
 
     # ---------------------------------------------------------------- plumbing
     def _check(self, st):
@@ -266,6 +277,33 @@ class Simulation:
         self._monitor_nf.append(len(f))
         return mid.value
 
+    def add_flux_monitor(self, k, freqs, dt=np.float32(0.05)):
+        """Poynting flux through the E plane z = k at each frequency (fdtd_add_flux_monitor):
+        six running DFTs (Ex, Ey at k; Hx, Hy at k-1 and k, phased half a step later)."""
+        f = np.ascontiguousarray(freqs, np.float64)
+        fid = C.c_int32()
+        self._check(self._L.fdtd_add_flux_monitor(self._h, int(k), _fp(f, C.c_double), len(f),
+                                                   float(np.float32(dt)), C.byref(fid)))
+        self.n_monitors += 6
+        self._monitor_nf += [len(f)] * 6
+        self._flux_nf.append(len(f))
+        return fid.value
+
+    def get_flux(self, flux_id):
+        out = np.empty(self._flux_nf[flux_id], np.float64)
+        self._check(self._L.fdtd_get_flux(self._h, int(flux_id), _fp(out, C.c_double)))
+        return out
+
+    def get_flux_device(self, flux_id, out_ptr, stream=None):
+        self._check(self._L.fdtd_get_flux_device(self._h, int(flux_id), C.c_void_p(out_ptr),
+                                                  _stream(stream)))
+
+    def flux_monitor_ids(self, flux_id):
+        """Monitor ids of Ex(k), Ey(k), Hx(k-1), Hx(k), Hy(k-1), Hy(k)."""
+        ids = (C.c_int32 * 6)()
+        self._check(self._L.fdtd_flux_monitor_ids(self._h, int(flux_id), ids))
+        return list(ids)
+
     # ---------------------------------------------------------------- running
     def reset(self):
         self._check(self._L.fdtd_reset(self._h))
@@ -297,6 +335,17 @@ class Simulation:
                 "tile_rows": out[2], "z_chunks": out[3], "launches": out[4],
                 "min_blocks": out[5], "dft_folds": folds.value}
 
+    def set_fast_path(self, enable):
+        """Uniform-material fast path of the tiled x-pair kernels (on by default); off forces
+        the general per-cell path, which gives the same bits."""
+        self._check(self._L.fdtd_set_fast_path(self._h, 1 if enable else 0))
+
+    @property
+    def fast_path(self):
+        v = C.c_int32()
+        self._check(self._L.fdtd_fast_path(self._h, C.byref(v)))
+        return bool(v.value)
+
     # ---------------------------------------------------------------- results
     def get_field(self, component, out=None):
         comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
@@ -318,6 +367,12 @@ class Simulation:
     def set_storage_scale(self, scale6):
         s = (C.c_float * 6)(*[float(v) for v in scale6])
         self._check(self._L.fdtd_set_storage_scale(self._h, s))
+        # the library keeps the nearest power of two of each (16-bit components only)
+        def p2(v):  # lround(log2 v): halves away from zero, as the library rounds
+            e = float(np.log2(float(v)))
+            return float(2.0 ** (np.floor(e + 0.5) if e >= 0 else -np.floor(-e + 0.5)))
+        self.storage_scale = [p2(v) if self.component_bytes(c) == 2 else 1.0
+                              for c, v in enumerate(scale6)]
 
     def set_field(self, component, values):
         comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)

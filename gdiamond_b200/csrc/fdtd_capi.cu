@@ -37,12 +37,22 @@ struct MonitorHost {
   long long k = 0;
   int nf = 0;
   double scale = 1.0, dt = 0.0;
+  double t_offset = 0.0;  // step t is phased at (t + t_offset) * dt (1/2 for a flux monitor's H)
   std::vector<double> freqs;
   double* re = nullptr;  // [nf][ny][nx]
   double* im = nullptr;
   double2* tab = nullptr;  // [tab_cap][nf]
   long long tab_cap = 0;
   float* stage = nullptr;  // [kDftSlots][ny][nx]: values the tiled kernels stage for the fold
+};
+
+// A flux monitor: six running DFTs (see flux.cu) and where its result goes.
+constexpr int kMaxFlux = fdtd::kMaxMonitors / 6;
+struct FluxHost {
+  long long k = 0;
+  int nf = 0;
+  int mon[6] = {};  // Ex(k), Ey(k), Hx(k-1), Hx(k), Hy(k-1), Hy(k)
+  double* out = nullptr;  // [nf] device result of the last reduction
 };
 
 std::string g_create_error;
@@ -86,6 +96,8 @@ struct fdtd_handle {
   long long tw = 0;
   MonitorHost mon[fdtd::kMaxMonitors];
   int nmon = 0;
+  FluxHost flux[kMaxFlux];
+  int nflux = 0;
   long long t = 0;
   int* d_err = nullptr;
   fdtd::TiledConfig cfg{0, 0, 0};
@@ -99,6 +111,12 @@ struct fdtd_handle {
   int esz = 4;     // bytes per stored field value (F16E: the FP16 E components')
   int nsets = 2;   // field sets (1 for FP64: the naive kernel updates in place)
   float scale[6] = {1, 1, 1, 1, 1, 1}, inv_scale[6] = {1, 1, 1, 1, 1, 1};
+  // Uniform-material fast path of the x-pair kernels (TiledArgs::lean): the dominant material
+  // qualifies when Ca = Da = 1 and Cb, Db are the same on all three axes.
+  bool lean_ok = false;
+  bool lean_enable = true;  // fdtd_set_fast_path
+  int lean_id = 0;
+  float lean_cb = 0.0f, lean_db = 0.0f;
   float* f32_stage = nullptr;   // pitched FP32 staging for field transfers of other storages
   double* f64_stage = nullptr;  // pitched FP64 staging for fdtd_get_field_f64
   std::string err;
@@ -242,7 +260,7 @@ fdtd_status ensure_tables(fdtd_handle* h, long long upto) {
     long long cap = std::max<long long>(upto, std::max<long long>(1024, mh.tab_cap * 2));
     std::vector<double2> host((size_t)cap * mh.nf);
     for (long long t = 0; t < cap; ++t) {
-      const double tt = (double)t * mh.dt;
+      const double tt = ((double)t + mh.t_offset) * mh.dt;
       for (int f = 0; f < mh.nf; ++f) {
         const double w = 2.0 * kPiD * mh.freqs[f];
         const double ph = w * tt;
@@ -282,6 +300,10 @@ fdtd::TiledArgs make_tiled_args(fdtd_handle* h, const fdtd::TiledConfig& c, long
     a.scale[k] = h->scale[k];
     a.inv_scale[k] = h->inv_scale[k];
   }
+  a.lean = h->lean_ok && h->lean_enable ? 1 : 0;
+  a.lean_id = h->lean_id;
+  a.lean_cb = h->lean_cb;
+  a.lean_db = h->lean_db;
   return a;
 }
 
@@ -407,8 +429,13 @@ fdtd_status check_device_error(fdtd_handle* h) {
   CUDA_TRY(h, cudaMemcpy(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (e != fdtd::kErrNone) {
     cudaMemset(h->d_err, 0, sizeof(int));
-    return fail(h, FDTD_ERR_DEVICE_TIMEOUT,
-                "a device-side bounded wait expired (error word %d); results are invalid", e);
+    if (e & fdtd::kErrTimeout)
+      return fail(h, FDTD_ERR_DEVICE_TIMEOUT,
+                  "a device-side bounded wait expired (error word %d); results are invalid", e);
+    return fail(h, FDTD_ERR_NUMERIC,
+                "a field value stored in 16 bits overflowed to +-inf or became NaN (error word "
+                "%d): the storage scale of that component is too small for the field; results "
+                "are invalid", e);
   }
   return FDTD_OK;
 }
@@ -430,6 +457,7 @@ void free_all(fdtd_handle* h) {
     cudaFree(h->mon[m].tab);
     cudaFree(h->mon[m].stage);
   }
+  for (int f = 0; f < h->nflux; ++f) cudaFree(h->flux[f].out);
   if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -481,9 +509,21 @@ fdtd_status compress_coefficients(fdtd_handle* h) {
   fdtd::DedupResult r{};
   CUDA_TRY(h, fdtd::build_material_map(h->g, h->coef, h->mat, h->table, h->scratch,
                                        fdtd::material_scratch_bytes(), h->stream, &r));
+  h->lean_ok = false;
   if (r.ok) {
     h->coef_mode = kCoefMaterial;
     h->nmat = r.nmat;
+    // Does the material held by the most cells qualify for the fast path?
+    Material m;
+    CUDA_TRY(h, cudaMemcpy(&m, h->table + r.dominant, sizeof(m), cudaMemcpyDeviceToHost));
+    // {Cax, Cbx, Cay, Cby}, {Caz, Cbz, Dax, Dbx}, {Day, Dby, Daz, Dbz}
+    const bool unit_a = m.a.x == 1.0f && m.a.z == 1.0f && m.b.x == 1.0f && m.b.z == 1.0f &&
+                        m.c.x == 1.0f && m.c.z == 1.0f;
+    const bool iso_b = m.a.y == m.a.w && m.a.y == m.b.y && m.b.w == m.c.y && m.b.w == m.c.w;
+    h->lean_ok = unit_a && iso_b;
+    h->lean_id = r.dominant;
+    h->lean_cb = m.a.y;
+    h->lean_db = m.b.w;
   } else {
     h->coef_mode = kCoefPerCell;
     h->nmat = 0;
@@ -494,6 +534,64 @@ fdtd_status compress_coefficients(fdtd_handle* h) {
 }  // namespace
 
 // ============================================================================== C-ABI
+
+namespace {
+
+// Adds one running-DFT monitor (fdtd_add_dft_monitor; a flux monitor adds six).
+fdtd_status add_monitor(fdtd_handle* h, int32_t component, int64_t k, const double* freqs,
+                        int32_t nf, double scale, double dt, double t_offset,
+                        int32_t* monitor_id) {
+  if (!h) return FDTD_ERR_INVALID_ARG;
+  if (h->nmon >= fdtd::kMaxMonitors)
+    return fail(h, FDTD_ERR_UNSUPPORTED, "at most %d monitors", fdtd::kMaxMonitors);
+  if (component < 0 || component > 5) return fail(h, FDTD_ERR_INVALID_ARG, "bad component");
+  if (k < 0 || k >= h->g.nz) return fail(h, FDTD_ERR_INVALID_ARG, "monitor plane outside grid");
+  if (!freqs || nf < 1 || nf > fdtd::kMaxFreqs)
+    return fail(h, FDTD_ERR_INVALID_ARG, "nf must be 1..%d", fdtd::kMaxFreqs);
+  DeviceGuard dg(h->desc.device);
+  MonitorHost& m = h->mon[h->nmon];
+  m = MonitorHost();
+  m.comp = component;
+  m.k = k;
+  m.nf = nf;
+  m.scale = scale;
+  m.dt = dt;
+  m.t_offset = t_offset;
+  m.freqs.assign(freqs, freqs + nf);
+  const size_t bytes = (size_t)nf * h->g.nx * h->g.ny * sizeof(double);
+  const size_t stage_bytes = (size_t)fdtd::kDftSlots * h->g.nx * h->g.ny * sizeof(float);
+  cudaError_t e = cudaMalloc(&m.re, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&m.im, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&m.stage, stage_bytes);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m.re, 0, bytes, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m.im, 0, bytes, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m.stage, 0, stage_bytes, h->stream);
+  if (e != cudaSuccess) {  // the monitor is not added: release what it had
+    cudaFree(m.re);
+    cudaFree(m.im);
+    cudaFree(m.stage);
+    m = MonitorHost();
+    return fail(h, e == cudaErrorMemoryAllocation ? FDTD_ERR_OOM : FDTD_ERR_CUDA,
+                "monitor allocation failed: %s", cudaGetErrorString(e));
+  }
+  if (monitor_id) *monitor_id = h->nmon;
+  h->nmon += 1;
+  return FDTD_OK;
+}
+
+// Removes the monitors from index `first` on (a flux monitor whose later parts failed).
+void drop_monitors(fdtd_handle* h, int first) {
+  for (int m = first; m < h->nmon; ++m) {
+    cudaFree(h->mon[m].re);
+    cudaFree(h->mon[m].im);
+    cudaFree(h->mon[m].tab);
+    cudaFree(h->mon[m].stage);
+    h->mon[m] = MonitorHost();
+  }
+  h->nmon = first;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -706,40 +804,74 @@ fdtd_status fdtd_set_sources(fdtd_handle* h, const fdtd_source* sources, int32_t
 fdtd_status fdtd_add_dft_monitor(fdtd_handle* h, int32_t component, int64_t k,
                                  const double* freqs, int32_t nf, double scale, double dt,
                                  int32_t* monitor_id) {
+  return add_monitor(h, component, k, freqs, nf, scale, dt, 0.0, monitor_id);
+}
+
+fdtd_status fdtd_add_flux_monitor(fdtd_handle* h, int64_t k, const double* freqs, int32_t nf,
+                                  double dt, int32_t* flux_id) {
   if (!h) return FDTD_ERR_INVALID_ARG;
-  if (h->nmon >= fdtd::kMaxMonitors)
-    return fail(h, FDTD_ERR_UNSUPPORTED, "at most %d monitors", fdtd::kMaxMonitors);
-  if (component < 0 || component > 5) return fail(h, FDTD_ERR_INVALID_ARG, "bad component");
-  if (k < 0 || k >= h->g.nz) return fail(h, FDTD_ERR_INVALID_ARG, "monitor plane outside grid");
-  if (!freqs || nf < 1 || nf > fdtd::kMaxFreqs)
-    return fail(h, FDTD_ERR_INVALID_ARG, "nf must be 1..%d", fdtd::kMaxFreqs);
-  DeviceGuard dg(h->desc.device);
-  MonitorHost& m = h->mon[h->nmon];
-  m = MonitorHost();
-  m.comp = component;
-  m.k = k;
-  m.nf = nf;
-  m.scale = scale;
-  m.dt = dt;
-  m.freqs.assign(freqs, freqs + nf);
-  const size_t bytes = (size_t)nf * h->g.nx * h->g.ny * sizeof(double);
-  const size_t stage_bytes = (size_t)fdtd::kDftSlots * h->g.nx * h->g.ny * sizeof(float);
-  cudaError_t e = cudaMalloc(&m.re, bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&m.im, bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&m.stage, stage_bytes);
-  if (e == cudaSuccess) e = cudaMemsetAsync(m.re, 0, bytes, h->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(m.im, 0, bytes, h->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(m.stage, 0, stage_bytes, h->stream);
-  if (e != cudaSuccess) {  // the monitor is not added: release what it had
-    cudaFree(m.re);
-    cudaFree(m.im);
-    cudaFree(m.stage);
-    m = MonitorHost();
-    return fail(h, e == cudaErrorMemoryAllocation ? FDTD_ERR_OOM : FDTD_ERR_CUDA,
-                "monitor allocation failed: %s", cudaGetErrorString(e));
+  if (h->nflux >= kMaxFlux)
+    return fail(h, FDTD_ERR_UNSUPPORTED, "at most %d flux monitors", kMaxFlux);
+  if (k < 1 || k > h->g.nz - 2)
+    return fail(h, FDTD_ERR_INVALID_ARG, "flux plane must be an interior plane 1..Nz-2");
+  if (h->nmon + 6 > fdtd::kMaxMonitors)
+    return fail(h, FDTD_ERR_UNSUPPORTED, "a flux monitor needs 6 of the %d monitor slots",
+                fdtd::kMaxMonitors);
+  FluxHost fx;
+  fx.k = k;
+  fx.nf = nf;
+  const int comps[6] = {FDTD_EX, FDTD_EY, FDTD_HX, FDTD_HX, FDTD_HY, FDTD_HY};
+  const int64_t planes[6] = {k, k, k - 1, k, k - 1, k};
+  const int first = h->nmon;
+  for (int q = 0; q < 6; ++q) {
+    fdtd_status s = add_monitor(h, comps[q], planes[q], freqs, nf, 1.0, dt,
+                                comps[q] >= FDTD_HX ? 0.5 : 0.0, &fx.mon[q]);
+    if (s != FDTD_OK) {
+      drop_monitors(h, first);
+      return s;
+    }
   }
-  if (monitor_id) *monitor_id = h->nmon;
-  h->nmon += 1;
+  DeviceGuard dg(h->desc.device);
+  if (cudaMalloc(&fx.out, (size_t)nf * sizeof(double)) != cudaSuccess) {
+    drop_monitors(h, first);
+    return fail(h, FDTD_ERR_OOM, "flux result allocation failed");
+  }
+  h->flux[h->nflux] = fx;
+  if (flux_id) *flux_id = h->nflux;
+  h->nflux += 1;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_get_flux_device(fdtd_handle* h, int32_t flux_id, double* flux_dev,
+                                 void* stream) {
+  if (!h || !flux_dev || flux_id < 0 || flux_id >= h->nflux) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  cudaStream_t st = pick_stream(h, stream);
+  const FluxHost& fx = h->flux[flux_id];
+  auto M = [&](int q) { return &h->mon[fx.mon[q]]; };
+  fdtd::FluxPlanes p{M(0)->re, M(0)->im, M(1)->re, M(1)->im, M(2)->re, M(2)->im,
+                     M(3)->re, M(3)->im, M(4)->re, M(4)->im, M(5)->re, M(5)->im};
+  const double dx = (double)h->desc.dx;
+  CUDA_TRY(h, fdtd::launch_flux_reduce(p, (long long)h->g.nx * h->g.ny, fx.nf, dx * dx,
+                                       flux_dev, st));
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_get_flux(fdtd_handle* h, int32_t flux_id, double* flux_out) {
+  if (!h || !flux_out || flux_id < 0 || flux_id >= h->nflux) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  FluxHost& fx = h->flux[flux_id];
+  fdtd_status s = fdtd_get_flux_device(h, flux_id, fx.out, nullptr);
+  if (s != FDTD_OK) return s;
+  CUDA_TRY(h, cudaMemcpyAsync(flux_out, fx.out, (size_t)fx.nf * sizeof(double),
+                              cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return check_device_error(h);
+}
+
+fdtd_status fdtd_flux_monitor_ids(const fdtd_handle* h, int32_t flux_id, int32_t* ids6) {
+  if (!h || !ids6 || flux_id < 0 || flux_id >= h->nflux) return FDTD_ERR_INVALID_ARG;
+  for (int q = 0; q < 6; ++q) ids6[q] = h->flux[flux_id].mon[q];
   return FDTD_OK;
 }
 
@@ -1040,6 +1172,18 @@ fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6) {
     h->scale[c] = std::ldexp(1.0f, e);
     h->inv_scale[c] = std::ldexp(1.0f, -e);
   }
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_set_fast_path(fdtd_handle* h, int32_t enable) {
+  if (!h) return FDTD_ERR_INVALID_ARG;
+  h->lean_enable = enable != 0;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_fast_path(const fdtd_handle* h, int32_t* active) {
+  if (!h || !active) return FDTD_ERR_INVALID_ARG;
+  *active = h->coef_mode == kCoefMaterial && h->lean_ok && h->lean_enable ? 1 : 0;
   return FDTD_OK;
 }
 

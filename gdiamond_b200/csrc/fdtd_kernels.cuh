@@ -41,6 +41,14 @@ struct TiledArgs {
   int* err;               // device error word
   float scale[6];         // 16-bit storage: value = stored * scale (powers of two)
   float inv_scale[6];
+  // Uniform-material path of the x-pair kernels: when lean != 0, material lean_id has
+  // Ca = Da = 1 on all three axes, Cb = lean_cb and Db = lean_db on all three (an isotropic
+  // lossless medium: vacuum or a dielectric).  A warp whose cells all carry that id (and lie
+  // away from sources) updates them with paired FP32 adds and the two coefficients from the
+  // parameters; 1*x == x, so the results are the general path's bit for bit.
+  int lean;
+  int lean_id;
+  float lean_cb, lean_db;
 };
 
 // A batch of grids for the persistent kernel: per-grid arguments (tensor maps included) in
@@ -111,6 +119,19 @@ cudaError_t launch_dft_fold(const Monitors& M, const Grid& g, long long t0, int 
 cudaError_t launch_dft_fold_batch(const TiledArgs* grids, int ngrids, long long max_np,
                                   int max_nf, long long t_offset, int n, cudaStream_t st);
 
+// ---------------------------------------------------------------- flux monitors (flux.cu)
+// The six running DFTs of a flux monitor on the E plane k ([nf][ny][nx] FP64 each): Ex, Ey of
+// plane k; Hx, Hy of planes k-1 (hx0, hy0) and k (hx1, hy1), phased at (t + 1/2) dt.
+struct FluxPlanes {
+  const double *ex_re, *ex_im, *ey_re, *ey_im;
+  const double *hx0_re, *hx0_im, *hx1_re, *hx1_im;
+  const double *hy0_re, *hy0_im, *hy1_re, *hy1_im;
+};
+// out_dev[f] = area * sum over the plane of Re[Ex conj(Hy) - Ey conj(Hx)], H averaged over the
+// two planes; np = nx * ny.
+cudaError_t launch_flux_reduce(const FluxPlanes& p, long long np, int nf, double area,
+                               double* out_dev, cudaStream_t st);
+
 // ---------------------------------------------------------------- coefficient builder
 struct Coef12Out {
   float* c[12];  // pitched per-cell arrays Cax..Dbz
@@ -125,6 +146,7 @@ cudaError_t build_coefficients(const Grid& g, const float* eps_dev, const float2
 struct DedupResult {
   int nmat;        // distinct 12-tuples (valid when ok)
   bool ok;         // false: more than 65536 materials, or a hash collision was detected
+  int dominant;    // id held by the most cells (valid when ok)
 };
 // coef12: 12 device arrays of nx*ny*nz floats (unpitched).  On success writes the pitched
 // material map and the table (capacity 65536 entries).

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(32 * TY) fdtd_tiled(const __grid_constant__ Ti
     const int stage = it % K::NS;
     if (!mbar_wait_bounded(&bars[stage], (uint32_t)(it / K::NS) & 1u, kWaitLimit)) {
       s_abort = 1;
-      atomicExch(a.err, kErrTimeout);
+      atomicOr(a.err, kErrTimeout);
     }
     if (B == 1) __syncthreads();  // orders last iteration's ebuf writes before this read
     const bool src_iter = smask != 0 && p >= src_lo && p <= src_hi;

@@ -1,0 +1,22 @@
+// k_tiled2_bf16.cu -- instances of the x-pair kernels (k_tiled2.cuh) for BF16 fields.
+#include "k_tiled2.cuh"
+
+namespace fdtd {
+
+cudaError_t tiled2_launch_bf16(const TiledConfig& c, const TiledArgs& a, dim3 grid,
+                               cudaStream_t st) {
+  return c.pairs32 ? launch_pairs32<__nv_bfloat16, __nv_bfloat16>(c.blt, c.rows, a, grid, st)
+                   : launch_type2<__nv_bfloat16, __nv_bfloat16>(c, a, grid, st);
+}
+
+cudaError_t tiled2_batch_launch_bf16(const TiledConfig& c, const BatchArgs& b, int ctas,
+                                     cudaStream_t st) {
+  return c.pairs32 ? launch_batch_pairs32<__nv_bfloat16, __nv_bfloat16>(c.blt, c.rows, b, ctas, st)
+                   : launch_batch_type<__nv_bfloat16, __nv_bfloat16>(c, b, ctas, st);
+}
+
+size_t tiled2_batch_query_bf16(const TiledConfig& c, bool occupancy) {
+  return occupancy ? batch_query<__nv_bfloat16, __nv_bfloat16, true>(c) : batch_query<__nv_bfloat16, __nv_bfloat16, false>(c);
+}
+
+}  // namespace fdtd

@@ -9,7 +9,9 @@
 //      64-bit keys; the thread that inserts a key records its cell as the representative;
 //   2. assign: number the occupied slots and copy each representative tuple into the table;
 //   3. map: write each cell's id and compare its 12 words with the table entry, so a 64-bit
-//      hash collision is detected (the map is then rejected) instead of silently merged.
+//      hash collision is detected (the map is then rejected) instead of silently merged; count
+//      the cells of each id and report the id held by the most cells (the kernels' fast path
+//      keeps that material's coefficients in registers).
 // Probing is bounded; overflow or more than 65536 tuples reject the map (the per-cell arrays
 // and the naive kernel are used instead).
 #include "fdtd_kernels.cuh"
@@ -31,6 +33,8 @@ struct Scratch {
   unsigned int nuniq;  // keys inserted
   unsigned int nid;    // ids handed out
   unsigned int flags;  // 1 = probe overflow, 2 = hash collision
+  unsigned int mode;   // id held by the most cells (the lowest such id on a tie)
+  unsigned int count[kMaxMaterials];  // cells per id
 };
 
 struct Coef12 {
@@ -66,7 +70,8 @@ __global__ void k_reset(Scratch* s) {
     s->rep[q] = kEmpty;
     s->ids[q] = 0xFFFFFFFFu;
   }
-  if (q == 0) s->nuniq = s->nid = s->flags = 0;
+  if (q < (uint32_t)kMaxMaterials) s->count[q] = 0;
+  if (q == 0) s->nuniq = s->nid = s->flags = s->mode = 0;
 }
 
 __global__ void k_insert(Grid g, Coef12 C, Scratch* s, long long n) {
@@ -144,6 +149,25 @@ __global__ void k_map(Grid g, Coef12 C, Scratch* s, const Material* table, uint1
     for (int a = 0; a < 12; ++a) same = same && (t[a] == w[a]);
     if (!same) atomicOr(&s->flags, 2u);
     mat[idx] = (uint16_t)id;
+    // cells per id: one atomic per group of lanes holding the same id
+    const unsigned peers = __match_any_sync(__activemask(), id);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s->count[id], __popc(peers));
+  }
+}
+
+// The id with the most cells (lowest id on a tie): one CTA of 1024 threads.
+__global__ void k_mode(Scratch* s, int nmat) {
+  __shared__ unsigned long long best[32];
+  unsigned long long b = 0;  // (count << 32) | (0xFFFFFFFF - id): max picks most cells, lowest id
+  for (int q = threadIdx.x; q < nmat; q += blockDim.x)
+    b = max(b, ((unsigned long long)s->count[q] << 32) | (0xFFFFFFFFu - (unsigned)q));
+  for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+  if ((threadIdx.x & 31) == 0) best[threadIdx.x >> 5] = b;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    b = best[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+    if (threadIdx.x == 0) s->mode = 0xFFFFFFFFu - (unsigned)(b & 0xFFFFFFFFu);
   }
 }
 
@@ -172,12 +196,15 @@ cudaError_t build_material_map(const Grid& g, const float* const* coef12, uint16
   if (hdr[2] != 0 || hdr[0] > (unsigned)kMaxMaterials) return cudaGetLastError();
   k_assign<<<(kSlots + threads - 1) / threads, threads, 0, st>>>(C, s, table);
   k_map<<<blocks, threads, 0, st>>>(g, C, s, table, mat, n);
-  if ((e = cudaMemcpyAsync(hdr, &s->nuniq, sizeof(hdr), cudaMemcpyDeviceToHost, st)) !=
+  k_mode<<<1, 1024, 0, st>>>(s, (int)hdr[0]);
+  unsigned int hdr4[4];
+  if ((e = cudaMemcpyAsync(hdr4, &s->nuniq, sizeof(hdr4), cudaMemcpyDeviceToHost, st)) !=
       cudaSuccess)
     return e;
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-  out->nmat = (int)hdr[0];
-  out->ok = hdr[2] == 0 && hdr[0] <= (unsigned)kMaxMaterials;
+  out->nmat = (int)hdr4[0];
+  out->ok = hdr4[2] == 0 && hdr4[0] <= (unsigned)kMaxMaterials;
+  out->dominant = (int)hdr4[3];
   return cudaGetLastError();
 }
 

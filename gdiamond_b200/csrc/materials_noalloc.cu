@@ -16,9 +16,14 @@
 //    the table and must be serialised by the caller.
 //  * In host code the array's name is only a host-side stand-in.  The first call on each
 //    device, with that device current, resolves its device address with cudaGetSymbolAddress
-//    (cached per device afterwards); make that first call before any stream capture.
+//    (cached per device afterwards).
 //  * No cudaMalloc, cudaFree or allocating library routine is called.  The call synchronises
-//    the given stream twice to read the table's counters into host variables.
+//    the given stream twice to read the table's counters into host variables, so it cannot be
+//    made on a stream that is being captured into a CUDA graph.
+//  * Ids are handed out in table-slot order by an atomic counter, so the numbering of the
+//    materials may differ from one call to the next; map and table are always consistent.
+//  * Data with more distinct tuples than the caller's table holds is rejected early: inserting
+//    threads stop once the count of distinct tuples passes max_materials.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -73,9 +78,14 @@ __global__ void na_clear(NaTable* s) {
   if (q == 0) s->nuniq = s->nid = s->flags = 0;
 }
 
-__global__ void na_insert(NaCoef C, NaTable* s, long long n) {
+// Inserts every cell's tuple; gives up (the call is rejected anyway) once more than
+// max_materials distinct tuples are in the table, checked before each cell and every 32 probes,
+// so data with many distinct tuples costs a short pass rather than full-table probes.
+__global__ void na_insert(NaCoef C, NaTable* s, long long n, int max_materials) {
+  const volatile unsigned int* nuniq = &s->nuniq;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
+    if (*nuniq > (unsigned)max_materials) return;
     uint32_t w[12];
 #pragma unroll
     for (int a = 0; a < 12; ++a) w[a] = __float_as_uint(C.c[a][i]);
@@ -96,6 +106,7 @@ __global__ void na_insert(NaCoef C, NaTable* s, long long n) {
         if (old == h) break;
       }
       slot = (slot + 1) & (kNaSlots - 1);
+      if ((probe & 31) == 31 && *nuniq > (unsigned)max_materials) return;
       if (probe == kNaMaxProbe - 1) atomicOr(&s->flags, 1u);
     }
   }
@@ -181,8 +192,11 @@ extern "C" fdtd_status fdtd_build_material_map_noalloc(const float* const* coef1
   for (int a = 0; a < 12; ++a) C.c[a] = coef12_dev[a];
   const long long n = (long long)nx * ny * nz;
   const int threads = 256, blocks = 148 * 8;
+  // A launch that fails leaves the table as the previous call left it, so its counters are
+  // only read after both launches of a pair were accepted.
   na_clear<<<(kNaSlots + threads - 1) / threads, threads, 0, st>>>(s);
-  na_insert<<<blocks, threads, 0, st>>>(C, s, n);
+  na_insert<<<blocks, threads, 0, st>>>(C, s, n, max_materials);
+  if (cudaPeekAtLastError() != cudaSuccess) return FDTD_ERR_CUDA;
   unsigned int hdr[3] = {0, 0, 0};
   if (cudaMemcpyAsync(hdr, &s->nuniq, sizeof(hdr), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
@@ -194,10 +208,10 @@ extern "C" fdtd_status fdtd_build_material_map_noalloc(const float* const* coef1
   na_assign<<<(kNaSlots + threads - 1) / threads, threads, 0, st>>>(C, s, table_dev,
                                                                      max_materials);
   na_map<<<blocks, threads, 0, st>>>(C, s, table_dev, mat_dev, n, max_materials);
+  if (cudaPeekAtLastError() != cudaSuccess) return FDTD_ERR_CUDA;
   if (cudaMemcpyAsync(hdr, &s->nuniq, sizeof(hdr), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return FDTD_ERR_CUDA;
-  if (cudaGetLastError() != cudaSuccess) return FDTD_ERR_CUDA;
   *nmat_out = (int32_t)hdr[0];
   return hdr[2] == 0 ? FDTD_OK : FDTD_ERR_UNSUPPORTED;
 }

@@ -19,17 +19,27 @@ from . import COMPONENTS
 
 
 def plane(sim, component="Ez", k=None):
-    """z-plane k (default Nz/2) of a component of the current field set: float32 [ny][nx]."""
+    """z-plane k (default Nz/2) of a component of the current field set: float32 [ny][nx].
+
+    Only that plane is copied out of the grid (raw storage values, Nx*Ny of them); 16-bit
+    values are widened and multiplied by their power-of-two storage scale, which is exact."""
     import torch
     nx, ny, nz = sim.shape
     k = nz // 2 if k is None else int(k)
     if not 0 <= k < nz:
         raise ValueError(f"plane {k} outside 0..{nz - 1}")
     comp = COMPONENTS.index(component) if isinstance(component, str) else int(component)
-    buf = torch.empty((nz, ny, nx), dtype=torch.float32, device=f"cuda:{sim._device}")
-    sim.get_field_device(comp, buf.data_ptr())
+    esz = sim.component_bytes(comp)
+    dtype = {4: torch.float32, 8: torch.float64}.get(esz)
+    if dtype is None:
+        dtype = torch.bfloat16 if sim.storage == "bf16" else torch.float16
+    raw = torch.empty((ny, nx), dtype=dtype, device=f"cuda:{sim._device}")
+    sim.get_planes_device(comp, k, 1, raw.data_ptr())
     sim.sync()
-    return buf[k].cpu().numpy()
+    out = raw.float()
+    if esz == 2:
+        out = out * sim.storage_scale[comp]
+    return out.cpu().numpy()
 
 
 def diverging_rgb(u, vmax):

@@ -150,12 +150,32 @@ fdtd_status fdtd_add_dft_monitor(fdtd_handle* h, int32_t component, int64_t k,
                                  const double* freqs, int32_t nf, double scale, double dt,
                                  int32_t* monitor_id);
 
+/* Poynting flux monitor on the E plane z = k (1 <= k <= Nz-2), at nf frequencies (FP64 Hz, in
+ * units of 1/dt's time unit), for a transmission spectrum.  The reference has no flux monitor,
+ * only the per-cell running DFT of one component (update_field_FFT_xy,
+ * gDiamond/kernels.cuh:87-113); this adds six such DFTs (monitor slots): Ex and Ey of plane k,
+ * Hx and Hy of planes k-1 and k.  Co-location: in the plane Ex and Hy share (i+1/2, j), Ey and Hx
+ * share (i, j+1/2); H is averaged over planes k-1 and k (z = k -+ 1/2).  Time: H of step t is
+ * phased at (t + 1/2) dt, E at t dt (Yee staggering).  fdtd_get_flux then gives, per frequency,
+ *   flux(f) = dx^2 * sum over the plane of Re[ Ex conj(Hy) - Ey conj(Hx) ]
+ * with X(f) = sum_t x(t) exp(-i 2 pi f t'), reduced on the GPU in FP64 (fixed order).
+ * fdtd_flux_monitor_ids gives the six monitor ids (their sums via fdtd_get_dft). */
+fdtd_status fdtd_add_flux_monitor(fdtd_handle* h, int64_t k, const double* freqs, int32_t nf,
+                                  double dt, int32_t* flux_id);
+fdtd_status fdtd_get_flux(fdtd_handle* h, int32_t flux_id, double* flux_out);
+/* Same into device memory (nf doubles), asynchronous on stream (or the handle's stream). */
+fdtd_status fdtd_get_flux_device(fdtd_handle* h, int32_t flux_id, double* flux_dev,
+                                 void* stream);
+fdtd_status fdtd_flux_monitor_ids(const fdtd_handle* h, int32_t flux_id, int32_t* ids6);
+
 /* Zeroes the fields and the monitor sums and sets the step counter to 0. */
 fdtd_status fdtd_reset(fdtd_handle* h);
 /* Runs T steps (asynchronous).  stream = a cudaStream_t, or NULL for the handle's stream. */
 fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream);
-/* Waits for the handle's work and reports any device-side error (e.g. a bounded wait that
- * gave up, FDTD_ERR_DEVICE_TIMEOUT). */
+/* Waits for the handle's work and reports any device-side error: a bounded wait that gave up
+ * (FDTD_ERR_DEVICE_TIMEOUT), or a field value stored in FP16/BF16 that overflowed to +-inf or
+ * became NaN because its storage scale is too small (FDTD_ERR_NUMERIC).  The reference has no
+ * error path here (CUDACHECK exits, gDiamond/gdiamond_gpu.cuh:11-20). */
 fdtd_status fdtd_sync(fdtd_handle* h);
 /* Global step counter (number of steps run since create/reset). */
 fdtd_status fdtd_get_step(const fdtd_handle* h, int64_t* t);
@@ -212,6 +232,17 @@ fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out6);
  * reference counterpart: gDiamond accumulates its monitors with one kernel per step. */
 fdtd_status fdtd_dft_folds(const fdtd_handle* h, int32_t* n);
 
+/* Uniform-material fast path of the tiled x-pair kernels (on by default).  When the material
+ * held by the most cells is isotropic and lossless (Ca = Da = 1, one Cb and one Db on all three
+ * axes: vacuum or a plain dielectric), warps whose cells all hold it, lie off the grid faces
+ * and hold no source update E' = E + Cb*curl H, H' = H + Db*curl E with paired FP32
+ * instructions and the two coefficients in registers.  Since 1*x == x the results are those of
+ * the general per-cell path bit for bit; enable = 0 forces the general path (for comparison).
+ * No reference counterpart: gDiamond reads all 12 coefficient arrays for every cell and step
+ * (gDiamond/kernels.cuh:337-394).  fdtd_fast_path reports whether the path is in use. */
+fdtd_status fdtd_set_fast_path(fdtd_handle* h, int32_t enable);
+fdtd_status fdtd_fast_path(const fdtd_handle* h, int32_t* active);
+
 /* Builds a material map from 12 device coefficient arrays without allocating anything.
  * No counterpart in the reference (which keeps 12 per-cell arrays); it is the allocation-free
  * form of the deduplication that fdtd_set_coefficients runs, for callers that cannot allocate
@@ -224,10 +255,12 @@ fdtd_status fdtd_dft_folds(const fdtd_handle* h, int32_t* n);
  *   nmat_out     out (host): number of distinct tuples found
  * Limit: at most 4096 distinct tuples; max_materials > 4096 is rejected with
  * FDTD_ERR_INVALID_ARG, data with more distinct tuples than max_materials with
- * FDTD_ERR_UNSUPPORTED.  The scratch is a fixed ~1.25 MB device array that every GPU loading the
- * library holds until exit; all calls share it (each clears it first), so calls that overlap
- * on the GPU race.  The first call on each device resolves that array's address; make it
- * before any stream capture.  The call synchronises `stream` (a cudaStream_t or NULL). */
+ * FDTD_ERR_UNSUPPORTED (such data is rejected after a short pass).  The scratch is a fixed
+ * ~1.25 MB device array that every GPU loading the library holds until exit; all calls share
+ * it (each clears it first), so calls that overlap on the GPU race.  The first call on each
+ * device resolves that array's address.  The call synchronises `stream` (a cudaStream_t or
+ * NULL), so it cannot be made on a stream that is being captured.  Ids follow table-slot order
+ * assigned by atomics: the numbering may differ between calls (map and table always agree). */
 fdtd_status fdtd_build_material_map_noalloc(const float* const* coef12_dev, int64_t nx,
                                             int64_t ny, int64_t nz, uint16_t* mat_dev,
                                             float* table_dev, int32_t max_materials,

@@ -35,7 +35,7 @@ namespace gdiamond {
 class gDiamond {
  public:
   enum Component { Ex = 0, Ey, Ez, Hx, Hy, Hz };
-  enum Variant { SEQ = 0, OMP = 1, GPU = 2, GPU_BL = 3 };
+  enum Variant { SEQ = 0, OMP = 1, GPU = 2, GPU_BL = 3, OMP_DT = 4 };
 
   // gDiamond/gdiamond.hpp:20-73: Nx*Ny*Nz grid, source at the centre cell, coefficients of a
   // vacuum box with a 10-cell graded pseudo-PML on every face.
@@ -71,6 +71,21 @@ class gDiamond {
 
   // gDiamond/gdiamond_omp.hpp:110-172: the same with `omp parallel for collapse(2)`.
   void update_FDTD_omp(size_t num_timesteps) { run_cpu(num_timesteps, OMP, true); }
+
+  // gDiamond/gdiamond_omp.hpp:174-261: the reference's temporally tiled OpenMP path, whose
+  // results equal update_FDTD_seq.  Here each block of BLT steps advances as a wavefront along z,
+  // in place: at wavefront position p, level s updates E of plane p-s+1 and then H of plane p-s,
+  // each plane's rows split over the OpenMP threads, so only the BLT planes in flight need to
+  // stay in cache.  Every cell sees the same operations in the same order as in seq (bit-equal
+  // results).  blx, bly and blz are the reference's spatial tile sizes; the plane wavefront has
+  // no spatial tiles, so they are accepted and not used.  Results -> OMP_DT.
+  void update_FDTD_omp_dt(size_t blx, size_t bly, size_t blz, size_t blt, size_t num_timesteps) {
+    (void)blx;
+    (void)bly;
+    (void)blz;
+    if (blt < 1) throw std::invalid_argument("BLT must be >= 1");
+    run_cpu_wavefront(num_timesteps, blt, OMP_DT);
+  }
 
   // ------------------------------------------------------------------ GPU paths (C-ABI)
   // gDiamond/gdiamond_gpu.cuh:483-648: per-step Mz source; results -> GPU.
@@ -126,6 +141,7 @@ class gDiamond {
   bool check_correctness_gpu_2D() const { return same(SEQ, GPU); }
   bool check_correctness_gpu() const { return same(GPU_BL, GPU); }
   bool check_correctness_omp() const { return same(SEQ, OMP); }
+  bool check_correctness_omp_dt() const { return same(SEQ, OMP_DT); }
 
   // ------------------------------------------------------------------ accessors
   const std::vector<float>& field(Component c, Variant v) const { return _res[v][c]; }
@@ -270,6 +286,65 @@ class gDiamond {
     for (int c = 0; c < 6; ++c) _res[v][c] = std::move(F[c]);
   }
 
+  // One plane of the E sweep / H sweep of run_cpu (rows split over OpenMP threads).
+  void e_plane(std::vector<float>* F, long k) const {
+    const long Nx = (long)_Nx, Ny = (long)_Ny;
+    const size_t sx = 1, sy = _Nx, sz = _Nx * _Ny;
+    float *Ex_ = F[0].data(), *Ey_ = F[1].data(), *Ez_ = F[2].data();
+    const float *Hx_ = F[3].data(), *Hy_ = F[4].data(), *Hz_ = F[5].data();
+    const float* const* C = _cptr;
+#pragma omp parallel for
+    for (long j = 1; j < Ny - 1; j++)
+      for (long i = 1; i < Nx - 1; i++) {
+        const size_t idx = i + j * sy + k * sz;
+        Ex_[idx] = C[0][idx] * Ex_[idx] + C[3][idx] * ((Hz_[idx] - Hz_[idx - sy]) - (Hy_[idx] - Hy_[idx - sz]));
+        Ey_[idx] = C[1][idx] * Ey_[idx] + C[4][idx] * ((Hx_[idx] - Hx_[idx - sz]) - (Hz_[idx] - Hz_[idx - sx]));
+        Ez_[idx] = C[2][idx] * Ez_[idx] + C[5][idx] * ((Hy_[idx] - Hy_[idx - sx]) - (Hx_[idx] - Hx_[idx - sy]));
+      }
+  }
+  void h_plane(std::vector<float>* F, long k, float mz) const {
+    const long Nx = (long)_Nx, Ny = (long)_Ny;
+    const size_t sx = 1, sy = _Nx, sz = _Nx * _Ny;
+    const float *Ex_ = F[0].data(), *Ey_ = F[1].data(), *Ez_ = F[2].data();
+    float *Hx_ = F[3].data(), *Hy_ = F[4].data(), *Hz_ = F[5].data();
+    const float* const* C = _cptr;
+#pragma omp parallel for
+    for (long j = 1; j < Ny - 1; j++)
+      for (long i = 1; i < Nx - 1; i++) {
+        const size_t idx = i + j * sy + k * sz;
+        float cz = (Ex_[idx + sy] - Ex_[idx]) - (Ey_[idx + sx] - Ey_[idx]);
+        if (idx == _source_idx) cz = cz - mz * _dx;
+        Hx_[idx] = C[6][idx] * Hx_[idx] + C[9][idx] * ((Ey_[idx + sz] - Ey_[idx]) - (Ez_[idx + sy] - Ez_[idx]));
+        Hy_[idx] = C[7][idx] * Hy_[idx] + C[10][idx] * ((Ez_[idx + sx] - Ez_[idx]) - (Ex_[idx + sz] - Ex_[idx]));
+        Hz_[idx] = C[8][idx] * Hz_[idx] + C[11][idx] * cz;
+      }
+  }
+
+  // Blocks of blt steps as an in-place z-wavefront (see update_FDTD_omp_dt).  E(e) at level s
+  // reads H(e) at level s-1 (updated earlier in this position by level s-1) and H(e-1) at level
+  // s-1 (advanced to level s only after E(e), in the same position); H(e-1) at level s reads
+  // E(e) and E(e-1) at level s (E(e-1) reaches level s+1 only after it).
+  void run_cpu_wavefront(size_t T, size_t blt, Variant v) {
+    const size_t n = cells();
+    std::vector<float> F[6];
+    for (auto& f : F) f.assign(n, 0.0f);
+    for (int a = 0; a < 12; ++a) _cptr[a] = _coef[a].data();
+    const long Nz = (long)_Nz;
+    for (size_t t0 = 0; t0 < T; t0 += blt) {
+      const long b = (long)std::min(blt, T - t0);
+      for (long p = 1; p <= Nz - 2 + b; ++p)
+        for (long s = 1; s <= b; ++s) {
+          const long e = p - s + 1, h = p - s;
+          if (e >= 1 && e <= Nz - 2) e_plane(F, e);
+          if (h >= 1 && h <= Nz - 2) {
+            const size_t t = t0 + (size_t)(s - 1);
+            h_plane(F, h, M_source_amp * std::sin(SOURCE_OMEGA * (float)t * dt));
+          }
+        }
+    }
+    for (int c = 0; c < 6; ++c) _res[v][c] = std::move(F[c]);
+  }
+
   void ensure_handle(int kernel) {
     if (_h && _h_kernel == kernel) return;
     if (_h) fdtd_destroy(_h);
@@ -337,7 +412,8 @@ class gDiamond {
   size_t _source_idx = 0;
   int _t_pml = 10;
   std::vector<float> _coef[12];
-  std::vector<float> _res[4][6];
+  std::vector<float> _res[5][6];
+  mutable const float* _cptr[12] = {};
   std::vector<double> _freqs, _dft_re, _dft_im;
   fdtd_handle* _h = nullptr;
   int _h_kernel = -1;

@@ -68,6 +68,8 @@ def lib():
         L.oracle_reference_mz_wave.argtypes = [C.c_int64, P(C.c_float)]
         L.oracle_dft_tables.argtypes = [P(C.c_double), C.c_int, C.c_double, C.c_int64,
                                         P(C.c_double), P(C.c_double)]
+        L.oracle_dft_tables_offset.argtypes = [P(C.c_double), C.c_int, C.c_double, C.c_double,
+                                               C.c_int64, P(C.c_double), P(C.c_double)]
         for name, T in (("oracle_run_f32", C.c_float), ("oracle_run_f64", C.c_double)):
             getattr(L, name).argtypes = [C.c_int64, C.c_int64, C.c_int64, P(P(T)),
                                          P(P(C.c_float)), C.c_float, P(_Source), C.c_int,
@@ -166,13 +168,15 @@ def reference_mz_wave(T):
     return out
 
 
-def dft_tables(freqs, dt, T):
+def dft_tables(freqs, dt, T, t_offset=0.0):
+    """cos / sin of (2 pi f) * ((t + t_offset) * dt) for t < T (t_offset 1/2: a flux monitor's
+    H fields)."""
     freqs = np.ascontiguousarray(freqs, np.float64)
     nf = len(freqs)
     ct = np.zeros((T, nf), np.float64)
     st = np.zeros((T, nf), np.float64)
-    lib().oracle_dft_tables(_fptr(freqs, C.c_double), nf, dt, T, _fptr(ct, C.c_double),
-                            _fptr(st, C.c_double))
+    lib().oracle_dft_tables_offset(_fptr(freqs, C.c_double), nf, dt, float(t_offset), T,
+                                   _fptr(ct, C.c_double), _fptr(st, C.c_double))
     return ct, st
 
 
@@ -194,6 +198,27 @@ class Monitor:
     scale: float = 1.0
     re: np.ndarray = field(default=None)
     im: np.ndarray = field(default=None)
+    t_offset: float = 0.0   # step t phased at (t + t_offset) dt
+
+
+def flux_monitors(k, freqs):
+    """The six running DFTs of a Poynting-flux monitor on the E plane z = k: Ex(k), Ey(k),
+    Hx(k-1), Hx(k), Hy(k-1), Hy(k), the H ones phased half a step later."""
+    return [Monitor("Ex", k, freqs), Monitor("Ey", k, freqs),
+            Monitor("Hx", k - 1, freqs, t_offset=0.5), Monitor("Hx", k, freqs, t_offset=0.5),
+            Monitor("Hy", k - 1, freqs, t_offset=0.5), Monitor("Hy", k, freqs, t_offset=0.5)]
+
+
+def flux(mons, dx):
+    """Flux spectrum from flux_monitors() after a run: per frequency
+    dx^2 * sum over the plane of Re[Ex conj(Hy) - Ey conj(Hx)], H averaged over the two planes
+    (k -+ 1/2 average to the E plane k); X = re + i im is the monitor's sum_t x(t) e^{-i w t'}.
+    There is no reference counterpart (the reference keeps a per-cell DFT of Ex only,
+    gDiamond/kernels.cuh:87-113); this is the definition the GPU reduction is checked against."""
+    ex, ey, hx0, hx1, hy0, hy1 = [m.re + 1j * m.im for m in mons]
+    hx, hy = 0.5 * (hx0 + hx1), 0.5 * (hy0 + hy1)
+    s = np.real(ex * np.conj(hy) - ey * np.conj(hx))
+    return float(dx) ** 2 * s.sum(axis=(1, 2))
 
 
 def run(shape, coefs, T, sources=(), monitors=(), dx=None, dt=None, fields=None, t0=0,
@@ -225,7 +250,7 @@ def run(shape, coefs, T, sources=(), monitors=(), dx=None, dt=None, fields=None,
     mon_arr = (_Monitor * max(len(monitors), 1))()
     for m_i, m in enumerate(monitors):
         freqs = np.asarray(m.freqs, np.float64)
-        ct, st = dft_tables(freqs, float(np.float32(dt)), t0 + T)
+        ct, st = dft_tables(freqs, float(np.float32(dt)), t0 + T, m.t_offset)
         if m.re is None:
             m.re = np.zeros((len(freqs), ny, nx), np.float64)
             m.im = np.zeros((len(freqs), ny, nx), np.float64)

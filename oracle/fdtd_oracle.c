@@ -136,8 +136,15 @@ void oracle_coefficients(int64_t Nx, int64_t Ny, int64_t Nz, float dx, float dt,
 
 void oracle_dft_tables(const double* freqs, int nf, double dt, int64_t T, double* cos_tab,
                        double* sin_tab) {
+  oracle_dft_tables_offset(freqs, nf, dt, 0.0, T, cos_tab, sin_tab);
+}
+
+/* The same with step t phased at (t + t_offset) * dt: t_offset = 1/2 for the H fields of a
+ * flux monitor (H of step t is half a step later than E of step t). */
+void oracle_dft_tables_offset(const double* freqs, int nf, double dt, double t_offset, int64_t T,
+                              double* cos_tab, double* sin_tab) {
   for (int64_t t = 0; t < T; ++t) {
-    const double tt = (double)t * dt;
+    const double tt = ((double)t + t_offset) * dt;
     for (int f = 0; f < nf; ++f) {
       const double w = 2.0 * PI_D * freqs[f];
       const double ph = w * tt;

@@ -61,6 +61,8 @@ void oracle_reference_params(float* out7, int* t_pml);
 void oracle_reference_mz_wave(int64_t T, float* out);
 
 /* FP64 cos/sin tables for the running DFT: ph = (2*pi*f) * ((double)t * dt), t = 0..T-1. */
+void oracle_dft_tables_offset(const double* freqs, int nf, double dt, double t_offset, int64_t T,
+                              double* cos_tab, double* sin_tab);
 void oracle_dft_tables(const double* freqs, int nf, double dt, int64_t T, double* cos_tab,
                        double* sin_tab);
 

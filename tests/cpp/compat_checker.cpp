@@ -1,8 +1,11 @@
-// The reference's unit tests (unittests/checker_gpu.cu, checker_omp.cpp) and example checks
+// The reference's unit tests (unittests/checker_gpu.cu, checker_omp.cpp, checker_omp_dt.cpp)
+// and example checks
 // (examples/gpu_mm_ver3.cu) written against include/gdiamond_compat.hpp.
 //
-//   compat_checker cpu Nx Ny Nz T [dump_prefix]   seq vs omp; optional raw dump of seq fields
+//   compat_checker cpu Nx Ny Nz T [dump_prefix]   seq vs omp and vs omp_dt (BLT 5 and 3);
+//                                                 optional raw dump of seq fields
 //   compat_checker gpu Nx Ny Nz T [dump_prefix]   seq vs gpu_2D, 3D-fix vs mix-mapping ver3,
+//                                                 ver3 vs the vectorized 3D-fix alias,
 //                                                 the figures path (Jx + Ex DFT)
 // Prints one JSON object; exit code 0 when every check holds.
 #include <cstdio>
@@ -44,22 +47,32 @@ int main(int argc, char** argv) {
   if (mode == "cpu") {
     exp.update_FDTD_omp(T);
     const bool omp_ok = exp.check_correctness_omp();
-    ok = ok && omp_ok;
-    std::printf(", \"omp_matches_seq\": %s", omp_ok ? "true" : "false");
+    exp.update_FDTD_omp_dt(16, 16, 16, 5, T);
+    const bool dt_ok = exp.check_correctness_omp_dt();
+    exp.update_FDTD_omp_dt(16, 16, 16, 3, T);
+    const bool dt3_ok = exp.check_correctness_omp_dt();
+    ok = ok && omp_ok && dt_ok && dt3_ok;
+    std::printf(", \"omp_matches_seq\": %s, \"omp_dt_matches_seq\": %s",
+                omp_ok ? "true" : "false", dt_ok && dt3_ok ? "true" : "false");
   } else {
     exp.update_FDTD_gpu_2D(T);
     const bool g2 = exp.check_correctness_gpu_2D();
     exp.update_FDTD_gpu_3D_warp_underutilization_fix(T);
     exp.update_FDTD_mix_mapping_gpu_ver3(T, 0, 0, 0);
     const bool g3 = exp.check_correctness_gpu();
+    // the float4 naive path's drop-in (gDiamond/gdiamond_gpu_naive_vectorized.cuh:28-181)
+    // writes the 3D-fix results, so ver3 vs it is the same check again
+    exp.update_FDTD_gpu_3D_warp_underutilization_fix_vectorized(T);
+    const bool gv = exp.check_correctness_gpu();
     exp.update_FDTD_gpu_figures(T);
     double dmax = 0;
     for (double v : exp.dft_real()) dmax = std::max(dmax, std::fabs(v));
     const bool figs = exp.dft_freqs().size() == 26 && dmax > 0 && std::isfinite(dmax);
-    ok = ok && g2 && g3 && figs;
-    std::printf(", \"gpu_2D_matches_seq\": %s, \"ver3_matches_3D_fix\": %s, \"figures_nf\": %zu, "
-                "\"figures_dft_max\": %.17g",
-                g2 ? "true" : "false", g3 ? "true" : "false", exp.dft_freqs().size(), dmax);
+    ok = ok && g2 && g3 && gv && figs;
+    std::printf(", \"gpu_2D_matches_seq\": %s, \"ver3_matches_3D_fix\": %s, "
+                "\"vectorized_matches_ver3\": %s, \"figures_nf\": %zu, \"figures_dft_max\": %.17g",
+                g2 ? "true" : "false", g3 ? "true" : "false", gv ? "true" : "false",
+                exp.dft_freqs().size(), dmax);
   }
   std::printf(", \"ok\": %s}\n", ok ? "true" : "false");
   return ok ? 0 : 1;

@@ -1,6 +1,7 @@
 """The C++ class surface (include/gdiamond_compat.hpp), compiled with g++ and run.
 
-Mirrors the reference's own tests: seq vs omp (unittests/checker_omp.cpp) on the CPU, and on
+Mirrors the reference's own tests: seq vs omp and omp_dt (unittests/checker_omp.cpp,
+checker_omp_dt.cpp) on the CPU, and on
 the GPU seq vs update_FDTD_gpu_2D (unittests/checker_gpu.cu) and the 3D-fix baseline vs
 mix-mapping ver3 (examples/gpu_mm_ver3.cu), all at the reference's |a-b| < 1e-8.  The seq
 fields are also checked bit for bit against the golden fixture generated from the reference.
@@ -40,7 +41,7 @@ def run(exe, *args):
 def test_cpp_seq_matches_golden_and_omp(checker, tmp_path):
     g = json.load(open(GOLDEN))
     rc, res = run(checker, "cpu", 100, 100, 100, 100, str(tmp_path / "seq_"))
-    assert rc == 0 and res["omp_matches_seq"]
+    assert rc == 0 and res["omp_matches_seq"] and res["omp_dt_matches_seq"]
     for c, n in enumerate(("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")):
         data = (tmp_path / f"seq_{c}.bin").read_bytes()
         assert hashlib.sha256(data).hexdigest() == g["seq"][n]["sha256"], n
@@ -51,5 +52,6 @@ def test_cpp_seq_matches_golden_and_omp(checker, tmp_path):
 def test_cpp_gpu_paths_match_reference_checks(checker):
     rc, res = run(checker, "gpu", 64, 56, 48, 90)
     assert res["gpu_2D_matches_seq"] and res["ver3_matches_3D_fix"]
+    assert res["vectorized_matches_ver3"]
     assert res["figures_nf"] == 26 and res["figures_dft_max"] > 0
     assert rc == 0

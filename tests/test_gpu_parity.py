@@ -10,8 +10,9 @@ failure reports both.  Cases:
   * every tiled (BLT, rows, z-chunks) instance on an odd grid with PML coefficients and J/M
     point sources; plane sources with random permittivity; FP64 DFT monitors;
   * per-cell coefficients that do not compress (naive fallback; tiled refused);
-  * at the full 256^3 x 1000 benchmark size: tiled == naive bit for bit, and linearity
-    (doubling the source doubles every field exactly);
+  * at the full 256^3 x 1000 benchmark size: the tiled kernel against the oracle bit for bit
+    (fields and the 8-frequency FP64 DFT), tiled == naive bit for bit, and linearity (doubling
+    the source doubles every field to FP32 rounding);
   * state handling: split step calls, reset, set_field.
 """
 import hashlib
@@ -229,6 +230,24 @@ def test_material_count_of_reference_constructor():
     sim.close()
 
 
+def test_full_size_benchmark_workload_against_oracle():
+    """The benchmark workload itself (256^3 vacuum, Gaussian Jz at the centre, 8-frequency FP64
+    DFT of Ez on z = 128, 1000 steps), autotuned tiled kernel against the oracle bit for bit."""
+    shape, T = (256, 256, 256), 1000
+    coefs = W.vacuum_coefficients(shape)
+    w = W.gaussian_wave(T)
+    freqs = W.source_band(8)
+    mons = [dict(component="Ez", k=128, freqs=freqs, scale=1.0)]
+    src = [dict(component="Jz", wave=w, i=128, j=128, k=128)]
+    F, D, cfg = gpu_run(shape, coefs, T, src, mons, kernel="auto")
+    assert cfg["kernel"] == "tiled"
+    om = oracle.Monitor("Ez", 128, freqs, 1.0)
+    F_ref = oracle.run(shape, coefs, T, sources=[osrc(s) for s in src], monitors=[om])
+    assert_fields_match(F, F_ref, "256^3 x 1000")
+    assert np.abs(om.re).max() > 0
+    assert np.array_equal(D[0][0], om.re) and np.array_equal(D[0][1], om.im)
+
+
 def test_full_size_tiled_equals_naive_and_is_linear():
     """256^3 x 1000 (the benchmark workload): size-independent properties."""
     shape, T = (256, 256, 256), 1000
@@ -309,7 +328,7 @@ def test_invalid_arguments_return_status():
     assert e.value.status == 1
     with pytest.raises(gd.FdtdError):
         sim.set_sources([dict(component="Jz", wave=np.ones(3, np.float32), i=25, j=1, k=1)])
-    for _ in range(4):
+    for _ in range(12):  # the monitor slots (a flux monitor takes six)
         sim.add_dft_monitor("Ez", 10, [1.0])
     with pytest.raises(gd.FdtdError) as e:
         sim.add_dft_monitor("Ez", 10, [1.0])

@@ -313,3 +313,35 @@ def test_batch_back_to_back_steps_without_sync():
         batch.close()
         for sim in sims:
             sim.close()
+
+
+@pytest.mark.parametrize("storage", ["f16", "f16e"])
+def test_16bit_overflow_is_reported_not_silent(storage):
+    """A storage scale far too small for the field makes stored FP16 values overflow (above
+    65504): fdtd_sync reports FDTD_ERR_NUMERIC instead of returning infinities silently.  After
+    a reset with a sound scale the handle steps correctly.  (BF16 has FP32's exponent range, so
+    it overflows only where FP32 would; the same check covers it.)"""
+    shape, T = (40, 32, 24), 30
+    coefs = W.reference_coefficients(shape)
+    w = W.gaussian_wave(T, delay=8.0, width=3.0, period=6.0)
+    src = [dict(component="Jz", wave=w, i=20, j=16, k=12)]
+    sim = gd.Simulation(*shape, storage=storage, blt=2)
+    sim.set_coefficients(coefs)
+    sim.set_sources(src)
+    sim.set_storage_scale([2.0 ** -20] * 6)
+    sim.step(T)
+    with pytest.raises(gd.FdtdError) as e:
+        sim.sync()
+    assert e.value.status == 6  # FDTD_ERR_NUMERIC
+    sim.sync()  # the error word was cleared with the report
+    # a sound scale: bit-exact against the oracle again
+    scales = [2.0, 2.0, 2.0, 0.5, 0.5, 0.5]
+    sim.set_storage_scale(scales)
+    sim.reset()
+    sim.step(T)
+    sim.sync()
+    F_ref = oracle_stored(shape, coefs, T, 2, storage, scales,
+                          [oracle.Source("Jz", w, i=20, j=16, k=12)], [])
+    for c, f in enumerate(sim.fields()):
+        assert bits_equal(f, F_ref[c]), (storage, c)
+    sim.close()

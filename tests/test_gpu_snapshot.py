@@ -38,3 +38,23 @@ def test_plane_and_png_match_oracle(tmp_path):
     with pytest.raises(ValueError):
         P.plane(sim, "Ez", nz)
     sim.close()
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16", "f16e"])
+def test_plane_of_16bit_storage_equals_the_full_field(storage):
+    """plane() copies one raw z-plane and widens it with the storage scale: the same values as
+    the whole-field conversion of the library, for scaled FP16 / BF16 and mixed F16E storage."""
+    shape, T = (40, 32, 24), 20
+    nx, ny, nz = shape
+    sim = gd.Simulation(*shape, storage=storage)
+    sim.set_storage_scale([4.0, 4.0, 4.0, 0.25, 0.25, 0.25])
+    sim.set_coefficients(W.reference_coefficients(shape))
+    w = W.gaussian_wave(T, delay=8.0, width=3.0, period=6.0)
+    sim.set_sources([dict(component="Jz", wave=w, i=20, j=16, k=12)])
+    sim.step(T)
+    for comp in ("Ex", "Ez", "Hy"):
+        got = P.plane(sim, comp, 12)
+        want = sim.get_field(comp).reshape(nz, ny, nx)[12]
+        assert np.abs(want).max() > 0
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (storage, comp)
+    sim.close()

@@ -71,7 +71,10 @@ def check_against_existing(coefs, shape):
     st, nmat, mat, table = noalloc(dev, shape, MAX_NOALLOC_MATERIALS)
     assert st == 0, gd.library().fdtd_status_string(st)
     assert nmat == expect
-    assert int(mat.max()) < nmat
+    # ids are dense (0..nmat-1 all used) and name distinct tuples; their numbering may differ
+    # from call to call, since ids follow table-slot order assigned by atomics
+    assert int(mat.max()) + 1 == nmat
+    assert len(np.unique(table[:nmat].view(np.uint32), axis=0)) == nmat
     for a in range(12):
         rebuilt = table[mat.astype(np.int64), a]
         assert np.array_equal(rebuilt.view(np.uint32),
@@ -95,3 +98,21 @@ def test_noalloc_rejects_sizes_beyond_its_limit():
     st, nmat, _, _ = noalloc(dev, shape, 16)
     assert st == 4 and nmat > 16  # FDTD_ERR_UNSUPPORTED: more tuples than the caller's table
     check_against_existing(W.reference_coefficients(shape), shape)  # still usable afterwards
+
+
+def test_noalloc_rejects_many_distinct_tuples_quickly():
+    """A graded medium with a distinct tuple per cell (far beyond the 4096 limit) is rejected
+    after a short pass: inserting stops once the count passes the caller's table size."""
+    import time
+    shape = (96, 96, 64)
+    n = int(np.prod(shape))
+    coefs = [c.copy() for c in W.vacuum_coefficients(shape)]
+    coefs[3] = (np.float32(0.25) + np.arange(n, dtype=np.float32) * np.float32(1e-7))  # Cbx
+    dev = to_device(coefs)
+    noalloc(dev, (8, 8, 8), MAX_NOALLOC_MATERIALS)  # first call on the device resolves the table
+    t0 = time.perf_counter()
+    st, nmat, _, _ = noalloc(dev, shape, MAX_NOALLOC_MATERIALS)
+    secs = time.perf_counter() - t0
+    assert st == 4 and nmat > MAX_NOALLOC_MATERIALS  # FDTD_ERR_UNSUPPORTED
+    assert secs < 2.0, secs
+    check_against_existing(W.vacuum_coefficients((40, 30, 20)), (40, 30, 20))  # still usable
