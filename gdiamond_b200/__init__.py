@@ -42,7 +42,7 @@ EXPORTS = (
     "fdtd_mlp_set_gemm", "fdtd_get_planes_device", "fdtd_set_planes_device",
     "fdtd_storage_bytes", "fdtd_set_step", "fdtd_set_dft", "fdtd_component_bytes",
     "fdtd_dft_folds", "fdtd_set_fast_path", "fdtd_fast_path", "fdtd_add_flux_monitor",
-    "fdtd_get_flux", "fdtd_get_flux_device", "fdtd_flux_monitor_ids",
+    "fdtd_get_flux", "fdtd_get_flux_device", "fdtd_flux_monitor_ids", "fdtd_debug_fail_copy",
 )
 
 
@@ -105,6 +105,8 @@ def library():
             "fdtd_component_bytes": ([V, C.c_int32, P(C.c_int32)], C.c_int),
             "fdtd_dft_folds": ([V, P(C.c_int32)], C.c_int),
             "fdtd_set_fast_path": ([V, C.c_int32], C.c_int),
+            "fdtd_debug_fail_copy": ([V, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64],
+                                     C.c_int),
             "fdtd_add_flux_monitor": ([V, C.c_int64, P(C.c_double), C.c_int32, C.c_double,
                                        P(C.c_int32)], C.c_int),
             "fdtd_get_flux": ([V, C.c_int32, P(C.c_double)], C.c_int),
@@ -339,6 +341,13 @@ class Simulation:
         """Uniform-material fast path of the tiled x-pair kernels (on by default); off forces
         the general per-cell path, which gives the same bits."""
         self._check(self._L.fdtd_set_fast_path(self._h, 1 if enable else 0))
+
+    def debug_fail_copy(self, tile, iteration, wait_cycles):
+        """Failure-path test hook (fdtd_debug_fail_copy): in the next tiled launch, tile
+        (bx, by, bz) skips the copy of one z-iteration and waits at most wait_cycles."""
+        bx, by, bz = (int(v) for v in tile)
+        self._check(self._L.fdtd_debug_fail_copy(self._h, bx, by, bz, int(iteration),
+                                                  int(wait_cycles)))
 
     @property
     def fast_path(self):

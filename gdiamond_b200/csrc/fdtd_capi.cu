@@ -113,6 +113,10 @@ struct fdtd_handle {
   float scale[6] = {1, 1, 1, 1, 1, 1}, inv_scale[6] = {1, 1, 1, 1, 1, 1};
   // Uniform-material fast path of the x-pair kernels (TiledArgs::lean): the dominant material
   // qualifies when Ca = Da = 1 and Cb, Db are the same on all three axes.
+  // fdtd_debug_fail_copy: applied to the next tiled launch only
+  int fault_tile[3] = {-1, -1, -1};
+  int fault_it = 0;
+  long long fault_wait = 0;
   bool lean_ok = false;
   bool lean_enable = true;  // fdtd_set_fast_path
   int lean_id = 0;
@@ -300,6 +304,13 @@ fdtd::TiledArgs make_tiled_args(fdtd_handle* h, const fdtd::TiledConfig& c, long
     a.scale[k] = h->scale[k];
     a.inv_scale[k] = h->inv_scale[k];
   }
+  // the failure-path test hook applies to stepping launches only (not to autotuning)
+  const bool hook = with_io && h->fault_tile[0] >= 0;
+  a.fault_bx = hook ? h->fault_tile[0] : -1;
+  a.fault_by = hook ? h->fault_tile[1] : -1;
+  a.fault_bz = hook ? h->fault_tile[2] : -1;
+  a.fault_it = h->fault_it;
+  a.wait_limit = hook ? h->fault_wait : 0;
   a.lean = h->lean_ok && h->lean_enable ? 1 : 0;
   a.lean_id = h->lean_id;
   a.lean_cb = h->lean_cb;
@@ -959,6 +970,7 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
         t_fold = h->t;
       }
       const fdtd::TiledArgs a = make_tiled_args(h, cc, h->t, true);
+      h->fault_tile[0] = h->fault_tile[1] = h->fault_tile[2] = -1;  // the hook fires once
       CUDA_TRY(h, launch_any(cc, a, h->g, st));
       ++launches;
       h->cur ^= 1;
@@ -1175,6 +1187,18 @@ fdtd_status fdtd_set_storage_scale(fdtd_handle* h, const float* scale6) {
   return FDTD_OK;
 }
 
+fdtd_status fdtd_debug_fail_copy(fdtd_handle* h, int32_t bx, int32_t by, int32_t bz,
+                                  int32_t iteration, int64_t wait_cycles) {
+  if (!h || bx < 0 || by < 0 || bz < 0 || iteration < 0 || wait_cycles < 1)
+    return FDTD_ERR_INVALID_ARG;
+  h->fault_tile[0] = bx;
+  h->fault_tile[1] = by;
+  h->fault_tile[2] = bz;
+  h->fault_it = iteration;
+  h->fault_wait = wait_cycles;
+  return FDTD_OK;
+}
+
 fdtd_status fdtd_set_fast_path(fdtd_handle* h, int32_t enable) {
   if (!h) return FDTD_ERR_INVALID_ARG;
   h->lean_enable = enable != 0;
@@ -1318,8 +1342,11 @@ void batch_fill_args(fdtd_batch* b, const fdtd::TiledConfig& c, bool with_io) {
     fdtd_handle* h = b->sims[i];
     fdtd::TiledConfig ci = c;
     ci.z_chunks = sim_chunks(h->g, b->zlen);
-    for (int p = 0; p < 2; ++p)
+    for (int p = 0; p < 2; ++p) {
       b->h_args[p * n + i] = make_tiled_args(h, ci, h->t, with_io, h->cur ^ p);
+      b->h_args[p * n + i].fault_bx = -1;  // the test hook is for single-grid steps
+      b->h_args[p * n + i].wait_limit = 0;
+    }
   }
 }
 

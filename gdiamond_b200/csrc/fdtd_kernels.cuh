@@ -49,6 +49,11 @@ struct TiledArgs {
   int lean;
   int lean_id;
   float lean_cb, lean_db;
+  // Failure-path test hook (fdtd_debug_fail_copy): tile (fault_bx, fault_by, fault_bz) does not
+  // issue the plane copy of its z-iteration fault_it (fault_bx = -1: no tile), and every bounded
+  // wait gives up after wait_limit SM clocks (0: about a second).
+  long long wait_limit;
+  int fault_bx, fault_by, fault_bz, fault_it;
 };
 
 // A batch of grids for the persistent kernel: per-grid arguments (tensor maps included) in

@@ -249,7 +249,10 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   for (int q = tid; q < (4 + 2 * B) * K::PLX; q += K::THREADS) hbuf[q] = 0.0f;
   __syncthreads();  // zeroed exchange planes; the previous tile's stages are all consumed
 
+  const long long wait_limit = a.wait_limit > 0 ? a.wait_limit : kWaitLimit;
+  const bool fault_tile = a.fault_bx == bx && a.fault_by == by && a.fault_bz == bz;
   auto issue = [&](int it_) {
+    if (fault_tile && it_ == a.fault_it) return;  // test hook: this copy is never issued
     const uint32_t u = gbase + (uint32_t)it_;
     const int stage = (int)(u % K::NS);
     uint64_t* bar = &bars[stage];
@@ -300,7 +303,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     const int p = ps + it;
     const uint32_t u = gbase + (uint32_t)it;
     const int stage = (int)(u % K::NS);
-    if (!mbar_wait_bounded(&bars[stage], (u / K::NS) & 1u, kWaitLimit)) {
+    if (!mbar_wait_bounded(&bars[stage], (u / K::NS) & 1u, wait_limit)) {
       *sm.abort = 1;
       atomicOr(a.err, kErrTimeout);
     }

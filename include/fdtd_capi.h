@@ -232,6 +232,17 @@ fdtd_status fdtd_get_config(const fdtd_handle* h, int32_t* out6);
  * reference counterpart: gDiamond accumulates its monitors with one kernel per step. */
 fdtd_status fdtd_dft_folds(const fdtd_handle* h, int32_t* n);
 
+/* Test hook for the failure path (no reference counterpart: the reference's CUDACHECK prints
+ * and exits, gDiamond/gdiamond_gpu.cuh:11-20).  In the next tiled fdtd_step launch only, tile
+ * (bx, by, bz) of the launch grid does not issue the shared-memory copy of its z-iteration
+ * `iteration`, and every bounded wait of that launch gives up after wait_cycles SM clocks
+ * instead of about a second.  The tile's wait for that copy then runs out: the tile leaves its
+ * z-march after its copies in flight have landed, nothing faults or hangs, and fdtd_sync returns
+ * FDTD_ERR_DEVICE_TIMEOUT (the fields are invalid; fdtd_reset makes the handle usable again).
+ * Single-grid steps only (not batches). */
+fdtd_status fdtd_debug_fail_copy(fdtd_handle* h, int32_t bx, int32_t by, int32_t bz,
+                                  int32_t iteration, int64_t wait_cycles);
+
 /* Uniform-material fast path of the tiled x-pair kernels (on by default).  When the material
  * held by the most cells is isotropic and lossless (Ca = Da = 1, one Cb and one Db on all three
  * axes: vacuum or a plain dielectric), warps whose cells all hold it, lie off the grid faces
