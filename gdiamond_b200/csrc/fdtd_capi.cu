@@ -117,6 +117,8 @@ struct fdtd_handle {
   int fault_tile[3] = {-1, -1, -1};
   int fault_it = 0;
   long long fault_wait = 0;
+  uint8_t* ublk = nullptr;  // uniform-block map of the lean material (fdtd::build_uniform_blocks)
+  int ub[3] = {0, 0, 0};
   bool lean_ok = false;
   bool lean_enable = true;  // fdtd_set_fast_path
   int lean_id = 0;
@@ -312,6 +314,10 @@ fdtd::TiledArgs make_tiled_args(fdtd_handle* h, const fdtd::TiledConfig& c, long
   a.fault_it = h->fault_it;
   a.wait_limit = hook ? h->fault_wait : 0;
   a.lean = h->lean_ok && h->lean_enable ? 1 : 0;
+  a.ublk = a.lean ? h->ublk : nullptr;
+  a.ubx = h->ub[0];
+  a.uby = h->ub[1];
+  a.ubz = h->ub[2];
   a.lean_id = h->lean_id;
   a.lean_cb = h->lean_cb;
   a.lean_db = h->lean_db;
@@ -460,6 +466,7 @@ void free_all(fdtd_handle* h) {
   cudaFree(h->scratch);
   cudaFree(h->d_wave);
   cudaFree(h->d_err);
+  cudaFree(h->ublk);
   cudaFree(h->f32_stage);
   cudaFree(h->f64_stage);
   for (int m = 0; m < h->nmon; ++m) {
@@ -535,6 +542,14 @@ fdtd_status compress_coefficients(fdtd_handle* h) {
     h->lean_id = r.dominant;
     h->lean_cb = m.a.y;
     h->lean_db = m.b.w;
+    if (h->lean_ok) {  // which blocks hold the lean material only (lean-only tiles)
+      h->ub[0] = (h->g.nx + fdtd::kUniX - 1) / fdtd::kUniX;
+      h->ub[1] = (h->g.ny + fdtd::kUniY - 1) / fdtd::kUniY;
+      h->ub[2] = (h->g.nz + fdtd::kUniZ - 1) / fdtd::kUniZ;
+      if (!h->ublk)
+        CUDA_TRY(h, cudaMalloc(&h->ublk, (size_t)h->ub[0] * h->ub[1] * h->ub[2]));
+      CUDA_TRY(h, fdtd::build_uniform_blocks(h->g, h->mat, r.dominant, h->ublk, h->stream));
+    }
   } else {
     h->coef_mode = kCoefPerCell;
     h->nmat = 0;

@@ -54,6 +54,12 @@ struct TiledArgs {
   // wait gives up after wait_limit SM clocks (0: about a second).
   long long wait_limit;
   int fault_bx, fault_by, fault_bz, fault_it;
+  // Uniform blocks for the lean-only z-march: ublk[(bz * uby + by) * ubx + bx] = 1 when every
+  // cell of the block of kUniX x kUniY cells by kUniZ planes holds material lean_id (null: no
+  // lean-only tiles).  A tile whose staged box touches only such blocks, and holds no source,
+  // runs every iteration on the lean path without loading or testing material planes.
+  const uint8_t* ublk;
+  int ubx, uby, ubz;
 };
 
 // A batch of grids for the persistent kernel: per-grid arguments (tensor maps included) in
@@ -146,6 +152,13 @@ struct Coef12Out {
 cudaError_t build_coefficients(const Grid& g, const float* eps_dev, const float2* sx,
                                const float2* sy, const float2* sz, float omega0, float dt,
                                float dx, const Coef12Out& out, cudaStream_t st);
+
+// ---------------------------------------------------------------- uniform blocks
+constexpr int kUniX = 8, kUniY = 8, kUniZ = 16;
+// out[(bz * nby + by) * nbx + bx] = 1 when every cell of the block holds material id `id`
+// (nbx = ceil(nx / kUniX) etc.; mat is the pitched material map).
+cudaError_t build_uniform_blocks(const Grid& g, const uint16_t* mat, int id, uint8_t* out,
+                                 cudaStream_t st);
 
 // ---------------------------------------------------------------- material dedup
 struct DedupResult {

@@ -169,14 +169,19 @@ struct Smem {
 //
 // Two forms of the per-level update, chosen per warp and z-iteration (warp-uniform, so the
 // barriers and shuffles stay common):
-//  * lean: every cell of the warp lies off the grid faces, carries material a.lean_id in all
-//    planes this iteration touches, and no source is in range.  Then Ca = Da = 1 and one Cb /
-//    Db for all axes, so E' = E + Cb*curl with paired FP32 instructions (sub/mul/add .f32x2)
-//    on the x-pair: 15 instructions per field and level for both cells;
+//  * lean: every cell of the warp carries material a.lean_id in all planes this iteration
+//    touches, no source is in range and the planes are off the z faces.  Then Ca = Da = 1 and
+//    one Cb / Db for all axes, so E' = E + Cb*curl: paired FP32 subtractions and additions
+//    (.f32x2) on the x-pair and separately rounded products; cells on an x or y face (or
+//    outside the grid) are restored by a select;
 //  * general: per-cell coefficients from the material table, face cells left unchanged,
 //    sources applied; separately rounded scalar arithmetic.
 // Both evaluate the same operations in the same order per cell, so they agree bit for bit.
-template <typename S, int B, int TY, int W = 64, typename SH = S>
+//
+// LO (lean only): the whole tile holds a.lean_id and no source (see tile_uniform), so every
+// iteration takes the lean path; the z faces are restored by the same select, and the material
+// planes are neither loaded nor tested.
+template <typename S, int B, int TY, int W = 64, typename SH = S, bool LO = false>
 __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz,
                                       const Smem& sm, uint32_t& gbase, long long t_offset) {
   using K = Tiled2<S, B, TY, W, SH>;
@@ -237,14 +242,17 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     sc[c] = scaled ? a.scale[c] : 1.0f;
     inv[c] = scaled ? a.inv_scale[c] : 1.0f;
   }
-  // Lean-path state, warp-uniform: wface = some cell of the warp lies on a grid face or outside
-  // the grid (the lean path then keeps those cells' values with a select); uh bit q = every
-  // cell of the warp in plane p-q holds lean_id.
+  // Lean-path state, warp-uniform: wface = some cell of the warp lies on an x or y face or
+  // outside the grid (the lean path then keeps those cells' values with a select); uh bit q =
+  // every cell of the warp in plane p-q holds lean_id.  Planes below the chunk's first loaded
+  // plane count as lean: what the warm-up computes there is discarded whatever the coefficients
+  // (outputs at planes >= z0 depend on loaded planes only), so the first iterations of a chunk
+  // need not take the general path.
   const bool lean_on = a.lean != 0;
   const bool wface = !__all_sync(kFull, int0 && int1);
   const uint32_t lean_ids = (uint32_t)a.lean_id * 0x10001u;
   constexpr uint32_t kPlanes = (1u << (B + 1)) - 1u;
-  uint32_t uh = 0;
+  uint32_t uh = ~0u;
 
   for (int q = tid; q < (4 + 2 * B) * K::PLX; q += K::THREADS) hbuf[q] = 0.0f;
   __syncthreads();  // zeroed exchange planes; the previous tile's stages are all consumed
@@ -256,7 +264,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
     const uint32_t u = gbase + (uint32_t)it_;
     const int stage = (int)(u % K::NS);
     uint64_t* bar = &bars[stage];
-    mbar_arrive_expect_tx(bar, K::TX_BYTES);
+    mbar_arrive_expect_tx(bar, LO ? K::STAGE_F_BYTES : K::TX_BYTES);
     unsigned char* d = st_f + stage * K::STAGE_F_BYTES;
     S* de = reinterpret_cast<S*>(d);
     SH* dh = reinterpret_cast<SH*>(d + K::OFF_HPLANES);
@@ -266,7 +274,7 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
       tma_load_3d(de + c * K::PL, &a.tm_src[c], bar, X8, Y, pz);
       tma_load_3d(dh + c * K::PL, &a.tm_src[3 + c], bar, X8, Y, pz);
     }
-    tma_load_3d(st_m + stage * K::MPL_S, &a.tm_mat, bar, X8, Y, pz);
+    if (!LO) tma_load_3d(st_m + stage * K::MPL_S, &a.tm_mat, bar, X8, Y, pz);
   };
   if (tid == 0) {
     fence_proxy_async_smem();
@@ -313,12 +321,14 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
 
     const S* E0 = reinterpret_cast<const S*>(st_f + stage * K::STAGE_F_BYTES);
     const SH* H0 = reinterpret_cast<const SH*>(st_f + stage * K::STAGE_F_BYTES + K::OFF_HPLANES);
+    bool lean = true;
+    if (!LO) {
 #pragma unroll
-    for (int s = B; s >= 1; --s) mq[s] = mq[s - 1];
-    mq[0] = *reinterpret_cast<const uint32_t*>(st_m + stage * K::MPL_S + om);
-    uh = (uh << 1) | (__all_sync(kFull, mq[0] == lean_ids) ? 1u : 0u);
-    const bool lean = lean_on && (uh & kPlanes) == kPlanes && p >= B + 1 && p <= g.nz - 2 &&
-                      !src_iter;
+      for (int s = B; s >= 1; --s) mq[s] = mq[s - 1];
+      mq[0] = *reinterpret_cast<const uint32_t*>(st_m + stage * K::MPL_S + om);
+      uh = (uh << 1) | (__all_sync(kFull, mq[0] == lean_ids) ? 1u : 0u);
+      lean = lean_on && (uh & kPlanes) == kPlanes && p >= B + 1 && p <= g.nz - 2 && !src_iter;
+    }
     float2 Hc[3], Eo[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -354,11 +364,13 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
         En[0] = add2(Eo[0], scale2(a.lean_cb, ex_c));
         En[1] = add2(Eo[1], scale2(a.lean_cb, ey_c));
         En[2] = add2(Eo[2], scale2(a.lean_cb, ez_c));
-        if (wface) {  // face and outside cells keep their value
+        const bool ke = !LO || (e >= 1 && e <= g.nz - 2);  // mixed tiles: lean only off z faces
+        if (wface || !ke) {  // face and outside cells keep their value
+          const bool u0 = int0 && ke, u1 = int1 && ke;
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            En[c].x = int0 ? En[c].x : Eo[c].x;
-            En[c].y = int1 ? En[c].y : Eo[c].y;
+            En[c].x = u0 ? En[c].x : Eo[c].x;
+            En[c].y = u1 ? En[c].y : Eo[c].y;
           }
         }
         const float2 ezxp = make_float2(Ep[s][2].y, ez_xp), eyxp = make_float2(Ep[s][1].y, ey_xp);
@@ -368,11 +380,13 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
         Hn[0] = add2(Hp[s - 1][0], scale2(a.lean_db, hx_c));
         Hn[1] = add2(Hp[s - 1][1], scale2(a.lean_db, hy_c));
         Hn[2] = add2(Hp[s - 1][2], scale2(a.lean_db, hz_c));
-        if (wface) {
+        const bool kh = !LO || (e - 1 >= 1 && e - 1 <= g.nz - 2);
+        if (wface || !kh) {
+          const bool u0 = int0 && kh, u1 = int1 && kh;
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            Hn[c].x = int0 ? Hn[c].x : Hp[s - 1][c].x;
-            Hn[c].y = int1 ? Hn[c].y : Hp[s - 1][c].y;
+            Hn[c].x = u0 ? Hn[c].x : Hp[s - 1][c].x;
+            Hn[c].y = u1 ? Hn[c].y : Hp[s - 1][c].y;
           }
         }
       } else {
@@ -559,6 +573,40 @@ __device__ __forceinline__ bool march(const TiledArgs& a, int bx, int by, int bz
   return true;
 }
 
+// Whether tile (bx, by, bz) of the grid in `a` may run the lean-only z-march: every in-grid cell
+// of its staged box over all planes it loads is in a uniform block of the lean material, and no
+// source lies in that box.  Cells outside the grid never change on the lean path either (a
+// select keeps them).  Every thread of the CTA calls it; the answer is CTA-uniform.
+template <typename S, int B, int TY, int W, typename SH>
+__device__ __forceinline__ bool tile_uniform(const TiledArgs& a, int bx, int by, int bz) {
+  using K = Tiled2<S, B, TY, W, SH>;
+  const Grid& g = a.g;
+  const int z0 = bz * a.zlen;
+  bool ok = a.ublk != nullptr && z0 < g.nz;
+  if (ok) {
+    const int X8 = (bx * K::SX + K::XBASE) & ~7, Y = by * K::SY - B;
+    const int za = max(0, z0 - B), zb = min(g.nz, min(g.nz, z0 + a.zlen) + B);  // [za, zb)
+    const int xa = max(0, X8), xb = min(g.nx, X8 + K::WB), ya = max(0, Y), yb = min(g.ny, Y + TY);
+    for (int n = 0; n < a.S.n; ++n) {
+      const SourceDev& s = a.S.s[n];
+      const bool in_z = s.k >= za - 1 && s.k <= zb;
+      if (in_z && (s.kind != 0 || (s.i >= xa && s.i < xb && s.j >= ya && s.j < yb))) ok = false;
+    }
+    if (ok && xa < xb && ya < yb) {
+      const int bx0 = xa / kUniX, bx1 = (xb - 1) / kUniX, by0 = ya / kUniY, by1 = (yb - 1) / kUniY;
+      const int bz0 = za / kUniZ, bz1 = (zb - 1) / kUniZ;
+      const int nxb = bx1 - bx0 + 1, nyb = by1 - by0 + 1;
+      const int nblk = nxb * nyb * (bz1 - bz0 + 1);
+      const int tid = threadIdx.y * 32 + threadIdx.x;
+      for (int q = tid; q < nblk; q += K::THREADS) {
+        const int qx = bx0 + q % nxb, qy = by0 + (q / nxb) % nyb, qz = bz0 + q / (nxb * nyb);
+        ok = ok && a.ublk[((long long)qz * a.uby + qy) * a.ubx + qx] != 0;
+      }
+    }
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
 template <typename S, int B, int TY, int W = 64, typename SH = S>
 __device__ __forceinline__ Smem setup_smem(unsigned char* smem_raw, int* s_abort) {
   using K = Tiled2<S, B, TY, W, SH>;
@@ -581,8 +629,11 @@ __global__ void __launch_bounds__(TY * W / 2, MINB)
   __shared__ int s_abort;
   const Smem sm = setup_smem<S, B, TY, W, SH>(smem_raw, &s_abort);
   uint32_t gbase = 0;
-  (void)march<S, B, TY, W, SH>(a, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, sm, gbase,
-                               0);
+  const int bx = (int)blockIdx.x, by = (int)blockIdx.y, bz = (int)blockIdx.z;
+  if (tile_uniform<S, B, TY, W, SH>(a, bx, by, bz))
+    (void)march<S, B, TY, W, SH, true>(a, bx, by, bz, sm, gbase, 0);
+  else
+    (void)march<S, B, TY, W, SH, false>(a, bx, by, bz, sm, gbase, 0);
 }
 
 // CTAs per SM the compiler must fit: two for the 24-row tiles of 32-cell rows (384 threads, the
@@ -610,7 +661,10 @@ __global__ void __launch_bounds__(TY * W / 2, (batch_min_blocks<TY, W>()))
     if (item >= b.nitems) break;
     const int4 w = b.items[item];  // {grid, bx, by, bz}
     const TiledArgs& a = b.grids[b.flip * b.ngrids + w.x];
-    if (!march<S, B, TY, W, SH>(a, w.y, w.z, w.w, sm, gbase, b.t_offset)) break;
+    const bool ok = tile_uniform<S, B, TY, W, SH>(a, w.y, w.z, w.w)
+                        ? march<S, B, TY, W, SH, true>(a, w.y, w.z, w.w, sm, gbase, b.t_offset)
+                        : march<S, B, TY, W, SH, false>(a, w.y, w.z, w.w, sm, gbase, b.t_offset);
+    if (!ok) break;
   }
 }
 

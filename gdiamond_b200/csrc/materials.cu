@@ -173,6 +173,39 @@ __global__ void k_mode(Scratch* s, int nmat) {
 
 }  // namespace
 
+namespace {
+
+// One warp per block of kUniX x kUniY x kUniZ cells: each lane tests 32 of its 1024 cells.
+__global__ void k_uniform_blocks(Grid g, const uint16_t* mat, int id, uint8_t* out, int nbx,
+                                 int nby, long long nblk) {
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+  const int lane = threadIdx.x & 31;
+  if (w >= nblk) return;  // warp-uniform
+  const int bx = (int)(w % nbx), by = (int)((w / nbx) % nby), bz = (int)(w / ((long long)nbx * nby));
+  bool ok = true;
+  for (int q = lane; q < kUniX * kUniY * kUniZ; q += 32) {
+    const int i = bx * kUniX + q % kUniX, j = by * kUniY + (q / kUniX) % kUniY;
+    const int k = bz * kUniZ + q / (kUniX * kUniY);
+    if (i < g.nx && j < g.ny && k < g.nz)
+      ok = ok && mat[i + (long long)j * g.pitch + (long long)k * g.plane] == (uint16_t)id;
+  }
+  ok = __all_sync(0xffffffffu, ok);
+  if (lane == 0) out[w] = ok ? 1 : 0;
+}
+
+}  // namespace
+
+cudaError_t build_uniform_blocks(const Grid& g, const uint16_t* mat, int id, uint8_t* out,
+                                 cudaStream_t st) {
+  const int nbx = (g.nx + kUniX - 1) / kUniX, nby = (g.ny + kUniY - 1) / kUniY;
+  const int nbz = (g.nz + kUniZ - 1) / kUniZ;
+  const long long nblk = (long long)nbx * nby * nbz;
+  const int threads = 256;
+  const long long blocks = (nblk * 32 + threads - 1) / threads;
+  k_uniform_blocks<<<(unsigned)blocks, threads, 0, st>>>(g, mat, id, out, nbx, nby, nblk);
+  return cudaGetLastError();
+}
+
 size_t material_scratch_bytes() { return sizeof(Scratch); }
 
 cudaError_t build_material_map(const Grid& g, const float* const* coef12, uint16_t* mat,
