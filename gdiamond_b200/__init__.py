@@ -43,6 +43,7 @@ EXPORTS = (
     "fdtd_storage_bytes", "fdtd_set_step", "fdtd_set_dft", "fdtd_component_bytes",
     "fdtd_dft_folds", "fdtd_set_fast_path", "fdtd_fast_path", "fdtd_add_flux_monitor",
     "fdtd_get_flux", "fdtd_get_flux_device", "fdtd_flux_monitor_ids", "fdtd_debug_fail_copy",
+    "fdtd_set_cpml", "fdtd_get_cpml_profile",
 )
 
 
@@ -57,6 +58,12 @@ class _Desc(C.Structure):
                 ("device", C.c_int32), ("storage", C.c_int32), ("kernel", C.c_int32),
                 ("blt", C.c_int32), ("tile_rows", C.c_int32), ("z_chunks", C.c_int32),
                 ("min_blocks", C.c_int32)]
+
+
+class _Cpml(C.Structure):
+    _fields_ = [("thickness", C.c_int32), ("faces", C.c_int32), ("order", C.c_float),
+                ("reflection", C.c_float), ("kappa_max", C.c_float), ("alpha_max", C.c_float),
+                ("dt", C.c_float)]
 
 
 class _Source(C.Structure):
@@ -105,6 +112,9 @@ def library():
             "fdtd_component_bytes": ([V, C.c_int32, P(C.c_int32)], C.c_int),
             "fdtd_dft_folds": ([V, P(C.c_int32)], C.c_int),
             "fdtd_set_fast_path": ([V, C.c_int32], C.c_int),
+            "fdtd_set_cpml": ([V, P(_Cpml)], C.c_int),
+            "fdtd_get_cpml_profile": ([V, C.c_int32, C.c_int32, P(C.c_float), P(C.c_float),
+                                       P(C.c_float), P(C.c_int32)], C.c_int),
             "fdtd_debug_fail_copy": ([V, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64],
                                      C.c_int),
             "fdtd_add_flux_monitor": ([V, C.c_int64, P(C.c_double), C.c_int32, C.c_double,
@@ -329,7 +339,7 @@ class Simulation:
     def config(self):
         out = (C.c_int32 * 6)()
         self._check(self._L.fdtd_get_config(self._h, out))
-        kernel = {1: "naive", 3: "tiled", 4: "tiled", 5: "tiled"}.get(out[0], "none")
+        kernel = {1: "naive", 3: "tiled", 4: "tiled", 5: "tiled", 6: "cpml"}.get(out[0], "none")
         width = {3: 32, 4: 64, 5: 32}.get(out[0], 0)
         folds = C.c_int32()
         self._check(self._L.fdtd_dft_folds(self._h, C.byref(folds)))
@@ -341,6 +351,30 @@ class Simulation:
         """Uniform-material fast path of the tiled x-pair kernels (on by default); off forces
         the general per-cell path, which gives the same bits."""
         self._check(self._L.fdtd_set_fast_path(self._h, 1 if enable else 0))
+
+    def set_cpml(self, thickness=10, faces=63, order=3.0, reflection=1e-6, kappa_max=1.0,
+                 alpha_max=0.05, dt=np.float32(0.05)):
+        """CPML absorbing layers (fdtd_set_cpml); thickness=None turns them off."""
+        if thickness is None:
+            self._check(self._L.fdtd_set_cpml(self._h, None))
+            return
+        d = _Cpml(int(thickness), int(faces), float(order), float(reflection), float(kappa_max),
+                  float(alpha_max), float(np.float32(dt)))
+        self._check(self._L.fdtd_set_cpml(self._h, C.byref(d)))
+
+    def cpml_tables(self):
+        """[axis][kind] = (slot, b, a, inv_kappa) of the layers (kind 0: E positions, 1: H)."""
+        out = []
+        for axis, n in enumerate(self.shape):
+            row = []
+            for kind in (0, 1):
+                b, a, ik = (np.empty(n, np.float32) for _ in range(3))
+                slot = np.empty(n, np.int32)
+                self._check(self._L.fdtd_get_cpml_profile(self._h, axis, kind, _fp(b), _fp(a),
+                                                           _fp(ik), _fp(slot, C.c_int32)))
+                row.append((slot, b, a, ik))
+            out.append(row)
+        return out
 
     def debug_fail_copy(self, tile, iteration, wait_cycles):
         """Failure-path test hook (fdtd_debug_fail_copy): in the next tiled launch, tile

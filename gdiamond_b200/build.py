@@ -18,7 +18,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libgdiamond_b200.so")
-SOURCES = ["fdtd_capi.cu", "k_naive.cu", "k_tiled.cu", "k_tiled2.cu", "k_tiled2_f32.cu", "k_tiled2_f16.cu", "k_tiled2_bf16.cu", "k_tiled2_f16e.cu", "convert.cu", "coefs.cu", "materials.cu", "materials_noalloc.cu", "mlp.cu", "mlp_tc.cu", "dft_fold.cu", "flux.cu"]
+SOURCES = ["fdtd_capi.cu", "k_naive.cu", "k_tiled.cu", "k_tiled2.cu", "k_tiled2_f32.cu", "k_tiled2_f16.cu", "k_tiled2_bf16.cu", "k_tiled2_f16e.cu", "convert.cu", "coefs.cu", "materials.cu", "materials_noalloc.cu", "mlp.cu", "mlp_tc.cu", "dft_fold.cu", "flux.cu", "cpml.cu"]
 HEADERS = ["fdtd_common.cuh", "fdtd_kernels.cuh", "k_tiled2.cuh", "mlp.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",

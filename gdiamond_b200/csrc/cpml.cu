@@ -1,0 +1,180 @@
+// cpml.cu -- convolutional PML (CPML) absorbing layers: per-step E and H kernels with the
+// auxiliary psi fields of the layers.
+//
+// The reference absorbs with a graded pseudo-PML folded into Ca/Cb/Da/Db (a real-valued
+// stretch, gDiamond/utils.h:585-660) in front of PEC faces that are never updated
+// (gDiamond/gdiamond.hpp:1193-1221); outgoing waves are partly reflected.  A CPML layer instead
+// replaces each spatial difference d in the curl by d / kappa + psi, with the recursive
+// convolution psi <- b psi + a d (complex-frequency-shifted stretch s = kappa + sigma /
+// (alpha + i w), in the normalised units of the reference: eps0 = mu0 = c = 1):
+//
+//   Ex <- Ca Ex + Cb [ (dyHz/ky + psi_exy) - (dzHy/kz + psi_exz) - Jx dx ],   dyHz = Hz(j) - Hz(j-1)
+//
+// and likewise for the other five components.  Profiles along each axis are tabulated at the E
+// positions (integer n) and the H positions (n + 1/2).  Outside every layer a component's update
+// is the reference's formula, operation for operation, so the interior stays bit-identical to
+// the non-PML solver; psi is stored only in the slabs of its axis (2 (L + 1) positions).
+#include "fdtd_kernels.cuh"
+
+namespace fdtd {
+
+namespace {
+
+struct CoefRefs {
+  const float* c[12];  // pitched per-cell arrays (or null with a material map)
+};
+
+__device__ __forceinline__ void e_coefs(const CoefRefs& A, const uint16_t* mat, const Material* tab,
+                                        long long idx, float* ca, float* cb) {
+  if (mat) {
+    const Material m = tab[mat[idx]];
+    ca[0] = m.a.x; cb[0] = m.a.y; ca[1] = m.a.z; cb[1] = m.a.w; ca[2] = m.b.x; cb[2] = m.b.y;
+  } else {
+    for (int c = 0; c < 3; ++c) {
+      ca[c] = A.c[c][idx];
+      cb[c] = A.c[3 + c][idx];
+    }
+  }
+}
+
+__device__ __forceinline__ void h_coefs(const CoefRefs& A, const uint16_t* mat, const Material* tab,
+                                        long long idx, float* da, float* db) {
+  if (mat) {
+    const Material m = tab[mat[idx]];
+    da[0] = m.b.z; db[0] = m.b.w; da[1] = m.c.x; db[1] = m.c.y; da[2] = m.c.z; db[2] = m.c.w;
+  } else {
+    for (int c = 0; c < 3; ++c) {
+      da[c] = A.c[6 + c][idx];
+      db[c] = A.c[9 + c][idx];
+    }
+  }
+}
+
+// psi slab element of axis a at slot s for cell (i, j, k)
+__device__ __forceinline__ long long psi_at(const Grid& g, int a, int S, int s, int i, int j, int k) {
+  if (a == 0) return s + (long long)S * (j + (long long)g.ny * k);
+  if (a == 1) return i + (long long)g.nx * (s + (long long)S * k);
+  return i + (long long)g.nx * (j + (long long)g.ny * s);
+}
+
+// The CPML form of one difference d along axis a at table position n: updates psi in place and
+// returns d / kappa + psi; outside the layer (slot < 0) returns d itself.
+__device__ __forceinline__ float stretched(float d, const CpmlAxis& ax, bool h, int n,
+                                           float* psi, long long pidx) {
+  const int s = h ? ax.slot_h[n] : ax.slot_e[n];
+  if (s < 0) return d;
+  const float b = h ? ax.bh[n] : ax.be[n], a = h ? ax.ah[n] : ax.ae[n];
+  const float ik = h ? ax.ikh[n] : ax.ike[n];
+  const float p = add(mul(b, psi[pidx]), mul(a, d));
+  psi[pidx] = p;
+  return add(mul(d, ik), p);
+}
+
+__device__ __forceinline__ bool src_sum(const Sources& S, int comp, int i, int j, int k,
+                                        long long t, float* v) {
+  return source_value(S, comp, i, j, k, t, v);
+}
+
+// grid (ceil(nx/32), ceil(ny/4), nz), block (32, 4); interior cells only, in place.
+__global__ void __launch_bounds__(128) cpml_e(Grid g, FieldPtrs F, CoefRefs A, const uint16_t* mat,
+                                              const Material* tab, Sources S, long long t,
+                                              float dx, CpmlDev P) {
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, k = blockIdx.z;
+  if (i < 1 || i > g.nx - 2 || j < 1 || j > g.ny - 2 || k < 1 || k > g.nz - 2) return;
+  const long long sy = g.pitch, sz = g.plane, idx = i + j * sy + k * sz;
+  float* const* f = F.f;
+  const float hx = f[3][idx], hy = f[4][idx], hz = f[5][idx];
+  const float dyHz = sub(hz, f[5][idx - sy]), dzHy = sub(hy, f[4][idx - sz]);
+  const float dzHx = sub(hx, f[3][idx - sz]), dxHz = sub(hz, f[5][idx - 1]);
+  const float dxHy = sub(hy, f[4][idx - 1]), dyHx = sub(hx, f[3][idx - sy]);
+  const CpmlAxis& X = P.ax[0];
+  const CpmlAxis& Y = P.ax[1];
+  const CpmlAxis& Z = P.ax[2];
+  float cx, cy, cz;
+  if (X.slot_e[i] < 0 && Y.slot_e[j] < 0 && Z.slot_e[k] < 0) {  // the reference's update
+    cx = sub(dyHz, dzHy);
+    cy = sub(dzHx, dxHz);
+    cz = sub(dxHy, dyHx);
+  } else {
+    const int sxs = X.slot_e[i] < 0 ? 0 : X.slot_e[i], sys = Y.slot_e[j] < 0 ? 0 : Y.slot_e[j];
+    const int szs = Z.slot_e[k] < 0 ? 0 : Z.slot_e[k];
+    cx = sub(stretched(dyHz, Y, false, j, P.psi_e[0], psi_at(g, 1, Y.S, sys, i, j, k)),
+             stretched(dzHy, Z, false, k, P.psi_e[1], psi_at(g, 2, Z.S, szs, i, j, k)));
+    cy = sub(stretched(dzHx, Z, false, k, P.psi_e[2], psi_at(g, 2, Z.S, szs, i, j, k)),
+             stretched(dxHz, X, false, i, P.psi_e[3], psi_at(g, 0, X.S, sxs, i, j, k)));
+    cz = sub(stretched(dxHy, X, false, i, P.psi_e[4], psi_at(g, 0, X.S, sxs, i, j, k)),
+             stretched(dyHx, Y, false, j, P.psi_e[5], psi_at(g, 1, Y.S, sys, i, j, k)));
+  }
+  if (S.n) {
+    float v;
+    if (src_sum(S, 0, i, j, k, t, &v)) cx = sub(cx, mul(v, dx));
+    if (src_sum(S, 1, i, j, k, t, &v)) cy = sub(cy, mul(v, dx));
+    if (src_sum(S, 2, i, j, k, t, &v)) cz = sub(cz, mul(v, dx));
+  }
+  float ca[3], cb[3];
+  e_coefs(A, mat, tab, idx, ca, cb);
+  f[0][idx] = yee(ca[0], f[0][idx], cb[0], cx);
+  f[1][idx] = yee(ca[1], f[1][idx], cb[1], cy);
+  f[2][idx] = yee(ca[2], f[2][idx], cb[2], cz);
+}
+
+__global__ void __launch_bounds__(128) cpml_h(Grid g, FieldPtrs F, CoefRefs A, const uint16_t* mat,
+                                              const Material* tab, Sources S, long long t,
+                                              float dx, CpmlDev P) {
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, k = blockIdx.z;
+  if (i < 1 || i > g.nx - 2 || j < 1 || j > g.ny - 2 || k < 1 || k > g.nz - 2) return;
+  const long long sy = g.pitch, sz = g.plane, idx = i + j * sy + k * sz;
+  float* const* f = F.f;
+  const float ex = f[0][idx], ey = f[1][idx], ez = f[2][idx];
+  const float dzEy = sub(f[1][idx + sz], ey), dyEz = sub(f[2][idx + sy], ez);
+  const float dxEz = sub(f[2][idx + 1], ez), dzEx = sub(f[0][idx + sz], ex);
+  const float dyEx = sub(f[0][idx + sy], ex), dxEy = sub(f[1][idx + 1], ey);
+  const CpmlAxis& X = P.ax[0];
+  const CpmlAxis& Y = P.ax[1];
+  const CpmlAxis& Z = P.ax[2];
+  float cx, cy, cz;
+  if (X.slot_h[i] < 0 && Y.slot_h[j] < 0 && Z.slot_h[k] < 0) {  // the reference's update
+    cx = sub(dzEy, dyEz);
+    cy = sub(dxEz, dzEx);
+    cz = sub(dyEx, dxEy);
+  } else {
+    const int sxs = X.slot_h[i] < 0 ? 0 : X.slot_h[i], sys = Y.slot_h[j] < 0 ? 0 : Y.slot_h[j];
+    const int szs = Z.slot_h[k] < 0 ? 0 : Z.slot_h[k];
+    cx = sub(stretched(dzEy, Z, true, k, P.psi_h[0], psi_at(g, 2, Z.S, szs, i, j, k)),
+             stretched(dyEz, Y, true, j, P.psi_h[1], psi_at(g, 1, Y.S, sys, i, j, k)));
+    cy = sub(stretched(dxEz, X, true, i, P.psi_h[2], psi_at(g, 0, X.S, sxs, i, j, k)),
+             stretched(dzEx, Z, true, k, P.psi_h[3], psi_at(g, 2, Z.S, szs, i, j, k)));
+    cz = sub(stretched(dyEx, Y, true, j, P.psi_h[4], psi_at(g, 1, Y.S, sys, i, j, k)),
+             stretched(dxEy, X, true, i, P.psi_h[5], psi_at(g, 0, X.S, sxs, i, j, k)));
+  }
+  if (S.n) {
+    float v;
+    if (src_sum(S, 3, i, j, k, t, &v)) cx = sub(cx, mul(v, dx));
+    if (src_sum(S, 4, i, j, k, t, &v)) cy = sub(cy, mul(v, dx));
+    if (src_sum(S, 5, i, j, k, t, &v)) cz = sub(cz, mul(v, dx));
+  }
+  float da[3], db[3];
+  h_coefs(A, mat, tab, idx, da, db);
+  f[3][idx] = yee(da[0], f[3][idx], db[0], cx);
+  f[4][idx] = yee(da[1], f[4][idx], db[1], cy);
+  f[5][idx] = yee(da[2], f[5][idx], db[2], cz);
+}
+
+}  // namespace
+
+cudaError_t launch_cpml_step(const Grid& g, const FieldPtrs& F, const float* const* coef,
+                             const uint16_t* mat, const Material* tab, const Sources& S,
+                             const Monitors& M, const CpmlDev& P, long long t, float dx,
+                             cudaStream_t st, int* launches) {
+  CoefRefs A;
+  for (int c = 0; c < 12; ++c) A.c[c] = coef ? coef[c] : nullptr;
+  const dim3 blk(32, 4), grd((g.nx + 31) / 32, (g.ny + 3) / 4, g.nz);
+  cpml_e<<<grd, blk, 0, st>>>(g, F, A, mat, tab, S, t, dx, P);
+  cpml_h<<<grd, blk, 0, st>>>(g, F, A, mat, tab, S, t, dx, P);
+  *launches += 2;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || M.n == 0) return e;
+  return launch_naive_dft(g, F, M, t, st, launches);
+}
+
+}  // namespace fdtd

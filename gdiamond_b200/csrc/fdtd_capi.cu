@@ -117,6 +117,14 @@ struct fdtd_handle {
   int fault_tile[3] = {-1, -1, -1};
   int fault_it = 0;
   long long fault_wait = 0;
+  // CPML layers (fdtd_set_cpml): per-axis tables in one device block, psi slab arrays
+  bool cpml_on = false;
+  fdtd_cpml_desc cpml{};
+  void* cpml_tab = nullptr;
+  float* cpml_psi[12] = {};
+  std::vector<int> cpml_slot[3][2];      // host copies of the slot tables (E, H positions)
+  std::vector<float> cpml_prof[3][2][3]; // host copies of b, a, 1/kappa
+  fdtd::CpmlDev cpml_dev{};
   uint8_t* ublk = nullptr;  // uniform-block map of the lean material (fdtd::build_uniform_blocks)
   int ub[3] = {0, 0, 0};
   bool lean_ok = false;
@@ -467,6 +475,8 @@ void free_all(fdtd_handle* h) {
   cudaFree(h->d_wave);
   cudaFree(h->d_err);
   cudaFree(h->ublk);
+  cudaFree(h->cpml_tab);
+  for (int q = 0; q < 12; ++q) cudaFree(h->cpml_psi[q]);
   cudaFree(h->f32_stage);
   cudaFree(h->f64_stage);
   for (int m = 0; m < h->nmon; ++m) {
@@ -605,6 +615,58 @@ fdtd_status add_monitor(fdtd_handle* h, int32_t component, int64_t k, const doub
   return FDTD_OK;
 }
 
+// Axis of the difference behind psi q (0..5: E exy exz eyz eyx ezx ezy; 6..11: H hxz hxy hyx
+// hyz hzy hzx).
+int cpml_psi_axis(int q) {
+  static const int ax[12] = {1, 2, 2, 0, 0, 1, 2, 1, 0, 2, 1, 0};
+  return ax[q];
+}
+
+size_t cpml_psi_bytes(const fdtd_handle* h, int q) {
+  const int a = cpml_psi_axis(q);
+  const size_t n[3] = {(size_t)h->g.nx, (size_t)h->g.ny, (size_t)h->g.nz};
+  const size_t S = 2 * (size_t)h->cpml.thickness + 1;
+  return S * n[(a + 1) % 3] * n[(a + 2) % 3] * sizeof(float);
+}
+
+// Profile of one axis at E positions (half = false: x = n) or H positions (x = n + 1/2).
+void cpml_profile(const fdtd_cpml_desc& d, int n, bool lo, bool hi, double dx, bool half,
+                  std::vector<int>* slot, std::vector<float>* b, std::vector<float>* a,
+                  std::vector<float>* ik) {
+  const int L = d.thickness;
+  const double m = d.order;
+  const double sigma_max = -(m + 1.0) * std::log((double)d.reflection) / (2.0 * L * dx);
+  slot->assign(n, -1);
+  b->assign(n, 1.0f);
+  a->assign(n, 0.0f);
+  ik->assign(n, 1.0f);
+  for (int p = 0; p < n; ++p) {
+    const double x = p + (half ? 0.5 : 0.0);
+    double rho = 0.0;
+    int s = -1;
+    if (lo && x < L) {
+      rho = (L - x) / L;
+      s = p;
+    }
+    if (hi && x > n - 1 - L) {
+      rho = (x - (n - 1 - L)) / L;
+      s = L + (p - (n - 1 - L));
+    }
+    if (!(rho > 0.0)) continue;
+    rho = std::min(rho, 1.0);
+    const double rm = std::pow(rho, m);
+    const double sigma = sigma_max * rm;
+    const double kappa = 1.0 + ((double)d.kappa_max - 1.0) * rm;
+    const double alpha = (double)d.alpha_max * (1.0 - rho);
+    const double bb = std::exp(-(sigma / kappa + alpha) * (double)d.dt);
+    const double den = sigma * kappa + kappa * kappa * alpha;
+    (*slot)[p] = s;
+    (*b)[p] = (float)bb;
+    (*a)[p] = den > 0.0 ? (float)(sigma / den * (bb - 1.0)) : 0.0f;
+    (*ik)[p] = (float)(1.0 / kappa);
+  }
+}
+
 // Removes the monitors from index `first` on (a flux monitor whose later parts failed).
 void drop_monitors(fdtd_handle* h, int first) {
   for (int m = first; m < h->nmon; ++m) {
@@ -732,13 +794,15 @@ fdtd_status fdtd_set_coefficients_device(fdtd_handle* h, const float* const* coe
 
 fdtd_status fdtd_set_permittivity(fdtd_handle* h, const float* eps_re, int32_t t_pml, float dt,
                                   float omega0) {
-  if (!h || t_pml < 1 || !(dt > 0) || !(omega0 > 0)) return FDTD_ERR_INVALID_ARG;
+  if (!h || t_pml < 0 || !(dt > 0) || !(omega0 > 0)) return FDTD_ERR_INVALID_ARG;
   DeviceGuard dg(h->desc.device);
   fdtd_status s = alloc_coef_staging(h);
   if (s != FDTD_OK) return s;
   const float dx = h->desc.dx;
   const float denom = 2 * 1.0f * (float)t_pml * dx;
-  const float sigma_max = (float)((double)(-4) * std::log(1e-5) / (double)denom);
+  // t_pml = 0: no graded layer (e.g. under CPML layers): every stretch factor is 1
+  const float sigma_max =
+      t_pml > 0 ? (float)((double)(-4) * std::log(1e-5) / (double)denom) : 0.0f;
   std::vector<float2> prof[3] = {stretch_profile(h->g.nx, t_pml, sigma_max, omega0),
                                  stretch_profile(h->g.ny, t_pml, sigma_max, omega0),
                                  stretch_profile(h->g.nz, t_pml, sigma_max, omega0)};
@@ -912,6 +976,10 @@ fdtd_status fdtd_reset(fdtd_handle* h) {
     CUDA_TRY(h, cudaMemsetAsync(h->mon[m].re, 0, bytes, h->stream));
     CUDA_TRY(h, cudaMemsetAsync(h->mon[m].im, 0, bytes, h->stream));
   }
+  if (h->cpml_on) {
+    for (int q = 0; q < 12; ++q)
+      CUDA_TRY(h, cudaMemsetAsync(h->cpml_psi[q], 0, cpml_psi_bytes(h, q), h->stream));
+  }
   h->t = 0;
   h->cur = 0;
   return FDTD_OK;
@@ -934,6 +1002,33 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
   }
   fdtd_status s = ensure_tables(h, h->t + T);
   if (s != FDTD_OK) return s;
+  if (h->cpml_on) {  // CPML layers: one E and one H kernel per step, monitors per step
+    if (h->storage != FDTD_STORE_F32)
+      return fail(h, FDTD_ERR_UNSUPPORTED, "CPML layers need FP32 field storage");
+    fdtd::FieldPtrs F;
+    for (int c = 0; c < 6; ++c) F.f[c] = h->F[h->cur][c];
+    const bool matm = h->coef_mode == kCoefMaterial;
+    const fdtd::Sources S = make_sources(h);
+    const fdtd::Monitors M = make_monitors(h);
+    int launches = 0;
+    for (int64_t q = 0; q < T; ++q) {
+      CUDA_TRY(h, fdtd::launch_cpml_step(h->g, F, matm ? nullptr : h->coef,
+                                         matm ? h->mat : nullptr, h->table, S, M, h->cpml_dev,
+                                         h->t, h->desc.dx, st, &launches));
+      h->t += 1;
+    }
+    h->last_kernel = 6;  // reported by fdtd_get_config: the per-step CPML kernels
+    h->last_launches = launches;
+    h->last_folds = 0;
+    if (st != h->stream) {
+      cudaEvent_t ev;
+      CUDA_TRY(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      CUDA_TRY(h, cudaEventRecord(ev, st));
+      CUDA_TRY(h, cudaStreamWaitEvent(h->stream, ev, 0));
+      cudaEventDestroy(ev);
+    }
+    return FDTD_OK;
+  }
   int kernel = h->desc.kernel;
   if (kernel == FDTD_KERNEL_AUTO)
     kernel = (h->coef_mode == kCoefMaterial && h->storage != FDTD_STORE_F64) ? FDTD_KERNEL_TILED
@@ -1211,6 +1306,90 @@ fdtd_status fdtd_debug_fail_copy(fdtd_handle* h, int32_t bx, int32_t by, int32_t
   h->fault_tile[2] = bz;
   h->fault_it = iteration;
   h->fault_wait = wait_cycles;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_set_cpml(fdtd_handle* h, const fdtd_cpml_desc* d) {
+  if (!h) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  cudaStreamSynchronize(h->stream);
+  cudaFree(h->cpml_tab);
+  h->cpml_tab = nullptr;
+  for (int q = 0; q < 12; ++q) {
+    cudaFree(h->cpml_psi[q]);
+    h->cpml_psi[q] = nullptr;
+  }
+  h->cpml_on = false;
+  if (!d) return FDTD_OK;
+  if (d->thickness < 1 || !(d->order >= 0) || !(d->reflection > 0 && d->reflection < 1) ||
+      !(d->kappa_max >= 1) || !(d->alpha_max >= 0) || !(d->dt > 0) || (d->faces & ~63))
+    return fail(h, FDTD_ERR_INVALID_ARG, "bad CPML description");
+  if (h->storage != FDTD_STORE_F32)
+    return fail(h, FDTD_ERR_UNSUPPORTED, "CPML layers need FP32 field storage");
+  const int n[3] = {h->g.nx, h->g.ny, h->g.nz};
+  for (int a = 0; a < 3; ++a)
+    if ((d->faces >> (2 * a) & 3) && n[a] < 2 * d->thickness + 2)
+      return fail(h, FDTD_ERR_INVALID_ARG, "axis %d has %d cells, CPML needs >= %d", a, n[a],
+                  2 * d->thickness + 2);
+  h->cpml = *d;
+  // tables: per axis and position kind, int slot[n] then b, a, 1/kappa [n] each
+  size_t bytes = 0;
+  for (int a = 0; a < 3; ++a) bytes += 2 * (size_t)n[a] * 16;
+  CUDA_TRY(h, cudaMalloc(&h->cpml_tab, bytes));
+  char* base = static_cast<char*>(h->cpml_tab);
+  size_t off = 0;
+  for (int a = 0; a < 3; ++a) {
+    fdtd::CpmlAxis& ax = h->cpml_dev.ax[a];
+    ax.S = 2 * d->thickness + 1;
+    for (int k = 0; k < 2; ++k) {
+      const bool lo = d->faces >> (2 * a) & 1, hi = d->faces >> (2 * a + 1) & 1;
+      auto& sl = h->cpml_slot[a][k];
+      auto* pr = h->cpml_prof[a][k];
+      cpml_profile(*d, n[a], lo, hi, (double)h->desc.dx, k == 1, &sl, &pr[0], &pr[1], &pr[2]);
+      int* d_slot = reinterpret_cast<int*>(base + off);
+      float* d_f = reinterpret_cast<float*>(base + off + (size_t)n[a] * 4);
+      CUDA_TRY(h, cudaMemcpy(d_slot, sl.data(), (size_t)n[a] * 4, cudaMemcpyHostToDevice));
+      for (int q = 0; q < 3; ++q)
+        CUDA_TRY(h, cudaMemcpy(d_f + (size_t)q * n[a], pr[q].data(), (size_t)n[a] * 4,
+                               cudaMemcpyHostToDevice));
+      if (k == 0) {
+        ax.slot_e = d_slot;
+        ax.be = d_f;
+        ax.ae = d_f + n[a];
+        ax.ike = d_f + 2 * (size_t)n[a];
+      } else {
+        ax.slot_h = d_slot;
+        ax.bh = d_f;
+        ax.ah = d_f + n[a];
+        ax.ikh = d_f + 2 * (size_t)n[a];
+      }
+      off += (size_t)n[a] * 16;
+    }
+  }
+  for (int q = 0; q < 12; ++q) {
+    const size_t pb = cpml_psi_bytes(h, q);
+    if (cudaMalloc(&h->cpml_psi[q], pb) != cudaSuccess) {
+      fdtd_set_cpml(h, nullptr);
+      return fail(h, FDTD_ERR_OOM, "CPML psi allocation failed");
+    }
+    CUDA_TRY(h, cudaMemset(h->cpml_psi[q], 0, pb));
+    (q < 6 ? h->cpml_dev.psi_e[q] : h->cpml_dev.psi_h[q - 6]) = h->cpml_psi[q];
+  }
+  h->cpml_on = true;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_get_cpml_profile(const fdtd_handle* h, int32_t axis, int32_t h_positions,
+                                  float* b, float* a, float* inv_kappa, int32_t* slot) {
+  if (!h || axis < 0 || axis > 2 || !h->cpml_on) return FDTD_ERR_INVALID_ARG;
+  const int k = h_positions ? 1 : 0;
+  const auto& pr = h->cpml_prof[axis][k];
+  const size_t n = pr[0].size();
+  if (b) std::copy(pr[0].begin(), pr[0].end(), b);
+  if (a) std::copy(pr[1].begin(), pr[1].end(), a);
+  if (inv_kappa) std::copy(pr[2].begin(), pr[2].end(), inv_kappa);
+  if (slot) std::copy(h->cpml_slot[axis][k].begin(), h->cpml_slot[axis][k].end(), slot);
+  (void)n;
   return FDTD_OK;
 }
 

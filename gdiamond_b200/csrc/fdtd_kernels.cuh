@@ -17,6 +17,34 @@ cudaError_t launch_naive_step(const Grid& g, const FieldPtrs& F, const float* co
                               const Monitors& M, long long t, float dx, cudaStream_t st,
                               int* launches, bool fp64);
 
+// Running-DFT update of every monitor from the current FP32 fields at step t (one launch).
+cudaError_t launch_naive_dft(const Grid& g, const FieldPtrs& F, const Monitors& M, long long t,
+                             cudaStream_t st, int* launches);
+
+// ---------------------------------------------------------------- CPML (cpml.cu)
+// One axis of the CPML profiles: tables over the n positions of the axis, at the E positions
+// (integer n: b, a, 1/kappa of the E updates' differences) and at the H positions (n + 1/2).
+// slot_* >= 0 inside a layer (the position's slot in the axis' psi slabs), -1 outside.
+struct CpmlAxis {
+  const int *slot_e, *slot_h;
+  const float *be, *ae, *ike;
+  const float *bh, *ah, *ikh;
+  int S;  // slots per axis
+};
+struct CpmlDev {
+  CpmlAxis ax[3];
+  // psi of the E updates: exy, exz, eyz, eyx, ezx, ezy; of the H updates: hxz, hxy, hyx, hyz,
+  // hzy, hzx (component, axis of the difference).  The array of axis a is a slab array: slot s
+  // of axis x at s + S*(j + ny*k); of y at i + nx*(s + S*k); of z at i + nx*(j + ny*s).
+  float* psi_e[6];
+  float* psi_h[6];
+};
+// One step of E then H with CPML layers (FP32 fields, in place), then the monitors.
+cudaError_t launch_cpml_step(const Grid& g, const FieldPtrs& F, const float* const* coef,
+                             const uint16_t* mat, const Material* tab, const Sources& S,
+                             const Monitors& M, const CpmlDev& P, long long t, float dx,
+                             cudaStream_t st, int* launches);
+
 // ---------------------------------------------------------------- storage conversion
 // Pitched field array of `storage` (0 FP32, 1 FP16, 2 BF16, 3 FP64) <-> pitched FP32 / FP64.
 cudaError_t convert_field_to_f32(const Grid& g, const void* src, int storage, float scale,

@@ -183,6 +183,15 @@ void naive_step_t(const Grid& g, const FieldPtrs& F, const CoefArrays& A, const 
   }
 }
 
+cudaError_t launch_naive_dft(const Grid& g, const FieldPtrs& F, const Monitors& M, long long t,
+                             cudaStream_t st, int* launches) {
+  if (M.n == 0) return cudaSuccess;
+  const dim3 b2(32, 8), g2((g.nx + 31) / 32, (g.ny + 7) / 8, M.n);
+  naive_dft<float><<<g2, b2, 0, st>>>(g, F, M, t);
+  *launches += 1;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_naive_step(const Grid& g, const FieldPtrs& F, const float* const* coef,
                               const uint16_t* mat, const Material* tab, const Sources& S,
                               const Monitors& M, long long t, float dx, cudaStream_t st,

@@ -105,7 +105,8 @@ def reference_coefficients(shape, eps_re=None, eps_im=None, dx=DX, dt=DT, omega0
     nx, ny, nz = shape
     a_max = np.float32(2.0)
     denom = np.float32(2) * np.float32(1.0) * np.float32(t_pml) * np.float32(dx)
-    sigma_max = np.float32(-4.0 * math.log(1e-5) / float(denom))
+    # t_pml = 0: no graded layer (e.g. under CPML layers), every stretch factor 1
+    sigma_max = np.float32(-4.0 * math.log(1e-5) / float(denom)) if t_pml > 0 else np.float32(0)
     sxr, sxi = _stretch_1d(nx, t_pml, a_max, sigma_max, omega0)
     syr, syi = _stretch_1d(ny, t_pml, a_max, sigma_max, omega0)
     szr, szi = _stretch_1d(nz, t_pml, a_max, sigma_max, omega0)

@@ -168,6 +168,36 @@ fdtd_status fdtd_get_flux_device(fdtd_handle* h, int32_t flux_id, double* flux_d
                                  void* stream);
 fdtd_status fdtd_flux_monitor_ids(const fdtd_handle* h, int32_t flux_id, int32_t* ids6);
 
+/* Convolutional PML (CPML) absorbing layers in place of the reference's graded pseudo-PML
+ * (gDiamond/utils.h:585-660, a real stretch folded into Ca/Cb/Da/Db in front of PEC faces).  In
+ * the layers every spatial difference d of the curl becomes d / kappa + psi with the recursive
+ * convolution psi <- b psi + a d, b = exp(-(sigma / kappa + alpha) dt),
+ * a = sigma (b - 1) / (sigma kappa + kappa^2 alpha), on the complex-frequency-shifted stretch
+ * s = kappa + sigma / (alpha + i w) (normalised units: eps0 = mu0 = c = 1).  Grading over the
+ * layer depth rho in [0, 1]: sigma = sigma_max rho^order with
+ * sigma_max = -(order + 1) ln(reflection) / (2 thickness dx), kappa = 1 + (kappa_max - 1)
+ * rho^order, alpha = alpha_max (1 - rho); E differences use rho at integer positions, H
+ * differences at half-integer ones.  Outside the layers the update is the reference's, bit for
+ * bit.  Give the interior material's coefficients (e.g. fdtd_set_permittivity with t_pml = 0):
+ * the CPML replaces the grading.  With layers on, fdtd_step runs one E and one H kernel per step
+ * (FP32 storage only); the psi fields live only in the slabs of their axis.  NULL turns the
+ * layers off. */
+typedef struct fdtd_cpml_desc {
+  int32_t thickness;   /* cells per face (L); each axis with layers needs >= 2 L + 2 cells */
+  int32_t faces;       /* bit mask of faces with a layer: 1 -x, 2 +x, 4 -y, 8 +y, 16 -z, 32 +z */
+  float order;         /* polynomial grading (3) */
+  float reflection;    /* normal-incidence reflection the grading aims at (1e-6) */
+  float kappa_max;     /* real stretch at the outer edge (1: none) */
+  float alpha_max;     /* CFS shift at the inner edge (0.05 in units of 1/time) */
+  float dt;            /* time step of the run (the reference's 0.05) */
+} fdtd_cpml_desc;
+fdtd_status fdtd_set_cpml(fdtd_handle* h, const fdtd_cpml_desc* desc);
+/* The tabulated profile of one axis (0 x, 1 y, 2 z) at E positions (h_positions = 0) or H
+ * positions (1): b, a, 1/kappa and the psi slot (-1 outside the layer), Nx/Ny/Nz entries each
+ * (any pointer may be NULL). */
+fdtd_status fdtd_get_cpml_profile(const fdtd_handle* h, int32_t axis, int32_t h_positions,
+                                  float* b, float* a, float* inv_kappa, int32_t* slot);
+
 /* Zeroes the fields and the monitor sums and sets the step counter to 0. */
 fdtd_status fdtd_reset(fdtd_handle* h);
 /* Runs T steps (asynchronous).  stream = a cudaStream_t, or NULL for the handle's stream. */
