@@ -127,6 +127,12 @@ struct fdtd_handle {
   fdtd::CpmlDev cpml_dev{};
   uint8_t* ublk = nullptr;  // uniform-block map of the lean material (fdtd::build_uniform_blocks)
   int ub[3] = {0, 0, 0};
+  std::vector<uint8_t> ublk_host;  // its host copy (tile launch order)
+  int* d_order = nullptr;          // tile launch order of the current configuration
+  size_t order_cap = 0;
+  std::vector<int> order_host;
+  long long order_key = -1;
+  int version = 0;                 // bumped when coefficients or sources change
   bool lean_ok = false;
   bool lean_enable = true;  // fdtd_set_fast_path
   int lean_id = 0;
@@ -475,6 +481,7 @@ void free_all(fdtd_handle* h) {
   cudaFree(h->d_wave);
   cudaFree(h->d_err);
   cudaFree(h->ublk);
+  cudaFree(h->d_order);
   cudaFree(h->cpml_tab);
   for (int q = 0; q < 12; ++q) cudaFree(h->cpml_psi[q]);
   cudaFree(h->f32_stage);
@@ -538,6 +545,8 @@ fdtd_status compress_coefficients(fdtd_handle* h) {
   CUDA_TRY(h, fdtd::build_material_map(h->g, h->coef, h->mat, h->table, h->scratch,
                                        fdtd::material_scratch_bytes(), h->stream, &r));
   h->lean_ok = false;
+  h->ublk_host.clear();
+  h->version += 1;
   if (r.ok) {
     h->coef_mode = kCoefMaterial;
     h->nmat = r.nmat;
@@ -559,6 +568,10 @@ fdtd_status compress_coefficients(fdtd_handle* h) {
       if (!h->ublk)
         CUDA_TRY(h, cudaMalloc(&h->ublk, (size_t)h->ub[0] * h->ub[1] * h->ub[2]));
       CUDA_TRY(h, fdtd::build_uniform_blocks(h->g, h->mat, r.dominant, h->ublk, h->stream));
+      h->ublk_host.resize((size_t)h->ub[0] * h->ub[1] * h->ub[2]);
+      CUDA_TRY(h, cudaMemcpyAsync(h->ublk_host.data(), h->ublk, h->ublk_host.size(),
+                                  cudaMemcpyDeviceToHost, h->stream));
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     }
   } else {
     h->coef_mode = kCoefPerCell;
@@ -665,6 +678,62 @@ void cpml_profile(const fdtd_cpml_desc& d, int n, bool lo, bool hi, double dx, b
     (*a)[p] = den > 0.0 ? (float)(sigma / den * (bb - 1.0)) : 0.0f;
     (*ik)[p] = (float)(1.0 / kappa);
   }
+}
+
+// Launch order of the tiles of x-pair configuration c (TiledArgs::tile_order): the tiles that
+// will run the mixed z-march (a source or a non-uniform block in their staged box; the device
+// test is tile_uniform in k_tiled2.cuh) first, then the lean-only ones.  Null when there is
+// nothing to reorder.
+const int* tile_order(fdtd_handle* h, const fdtd::TiledConfig& c) {
+  if (!(c.width == 64 || c.pairs32) || h->ublk_host.empty() || !h->lean_enable) return nullptr;
+  const long long key = ((((long long)h->version * 8 + c.blt) * 64 + c.rows) * 64 + c.z_chunks) *
+                            2 + (c.pairs32 ? 1 : 0) + 4LL * c.width;
+  if (key == h->order_key) return h->d_order;
+  const Grid& g = h->g;
+  const int W = c.pairs32 ? 32 : c.width, B = c.blt;
+  const int SX = fdtd::tiled2_sx_w(W, B), SY = fdtd::tiled_sy(B, c.rows);
+  const int XB = fdtd::tiled2_xbase(B), WB = W + fdtd::kTiled2BoxPad;
+  const int zlen = (g.nz + c.z_chunks - 1) / c.z_chunks;
+  const dim3 gd = fdtd::tiled2_grid(c, g);
+  const int ntile = (int)(gd.x * gd.y * gd.z);
+  std::vector<int> mixed, lean;
+  for (int q = 0; q < ntile; ++q) {
+    const int bx = q % gd.x, by = (q / gd.x) % gd.y, bz = q / (gd.x * gd.y);
+    const int z0 = bz * zlen, X8 = (bx * SX + XB) & ~7, Y = by * SY - B;
+    const int za = std::max(0, z0 - B), zb = std::min(g.nz, std::min(g.nz, z0 + zlen) + B);
+    const int xa = std::max(0, X8), xb = std::min(g.nx, X8 + WB);
+    const int ya = std::max(0, Y), yb = std::min(g.ny, Y + c.rows);
+    bool ok = true;
+    for (int n = 0; n < h->nsrc && ok; ++n) {
+      const fdtd::SourceDev& sd = h->src[n];
+      const bool in_z = sd.k >= za - 1 && sd.k <= zb;
+      if (in_z && (sd.kind != 0 || (sd.i >= xa && sd.i < xb && sd.j >= ya && sd.j < yb))) ok = false;
+    }
+    if (ok && xa < xb && ya < yb)
+      for (int kz = za / fdtd::kUniZ; ok && kz <= (zb - 1) / fdtd::kUniZ; ++kz)
+        for (int ky = ya / fdtd::kUniY; ok && ky <= (yb - 1) / fdtd::kUniY; ++ky)
+          for (int kx = xa / fdtd::kUniX; ok && kx <= (xb - 1) / fdtd::kUniX; ++kx)
+            ok = h->ublk_host[((size_t)kz * h->ub[1] + ky) * h->ub[0] + kx] != 0;
+    (ok ? lean : mixed).push_back(q);
+  }
+  h->order_key = key;
+  if (mixed.empty() || lean.empty()) {
+    h->order_host.clear();
+    return nullptr;
+  }
+  h->order_host = mixed;
+  h->order_host.insert(h->order_host.end(), lean.begin(), lean.end());
+  if (h->order_cap < (size_t)ntile) {
+    cudaFree(h->d_order);
+    h->d_order = nullptr;
+    h->order_cap = 0;
+    if (cudaMalloc(&h->d_order, (size_t)ntile * sizeof(int)) != cudaSuccess) return nullptr;
+    h->order_cap = ntile;
+  }
+  if (cudaMemcpy(h->d_order, h->order_host.data(), (size_t)ntile * sizeof(int),
+                 cudaMemcpyHostToDevice) != cudaSuccess)
+    return nullptr;
+  return h->d_order;
 }
 
 // Removes the monitors from index `first` on (a flux monitor whose later parts failed).
@@ -888,6 +957,7 @@ fdtd_status fdtd_set_sources(fdtd_handle* h, const fdtd_source* sources, int32_t
   }
   h->nsrc = nsrc;
   h->tw = T_wave;
+  h->version += 1;
   return FDTD_OK;
 }
 
@@ -1068,6 +1138,7 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
     // complete whenever fdtd_step returns.
     long long t_fold = h->t;
     int64_t left = T;
+    const int* order = tile_order(h, c);
     while (left > 0) {
       fdtd::TiledConfig cc = c;
       if (left < c.blt) {  // a shorter final pass (plain register allocation)
@@ -1079,7 +1150,8 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
         ++folds;
         t_fold = h->t;
       }
-      const fdtd::TiledArgs a = make_tiled_args(h, cc, h->t, true);
+      fdtd::TiledArgs a = make_tiled_args(h, cc, h->t, true);
+      a.tile_order = cc.blt == c.blt ? order : nullptr;
       h->fault_tile[0] = h->fault_tile[1] = h->fault_tile[2] = -1;  // the hook fires once
       CUDA_TRY(h, launch_any(cc, a, h->g, st));
       ++launches;

@@ -88,6 +88,11 @@ struct TiledArgs {
   // runs every iteration on the lean path without loading or testing material planes.
   const uint8_t* ublk;
   int ubx, uby, ubz;
+  // Launch order of the tiles (single-grid launches): CTA q of the grid (x fastest) runs tile
+  // tile_order[q] (linear index bx + ntx * (by + nty * bz)); null: CTA q runs tile q.  The host
+  // puts the tiles that cannot take the lean-only march (sources, mixed materials) first, so
+  // the slower CTAs start in the first wave instead of lengthening the last one.
+  const int* tile_order;
 };
 
 // A batch of grids for the persistent kernel: per-grid arguments (tensor maps included) in

@@ -629,7 +629,13 @@ __global__ void __launch_bounds__(TY * W / 2, MINB)
   __shared__ int s_abort;
   const Smem sm = setup_smem<S, B, TY, W, SH>(smem_raw, &s_abort);
   uint32_t gbase = 0;
-  const int bx = (int)blockIdx.x, by = (int)blockIdx.y, bz = (int)blockIdx.z;
+  int bx = (int)blockIdx.x, by = (int)blockIdx.y, bz = (int)blockIdx.z;
+  if (a.tile_order) {
+    const int q = a.tile_order[bx + (int)gridDim.x * (by + (int)gridDim.y * bz)];
+    bx = q % (int)gridDim.x;
+    by = (q / (int)gridDim.x) % (int)gridDim.y;
+    bz = q / ((int)gridDim.x * (int)gridDim.y);
+  }
   if (tile_uniform<S, B, TY, W, SH>(a, bx, by, bz))
     (void)march<S, B, TY, W, SH, true>(a, bx, by, bz, sm, gbase, 0);
   else

@@ -280,6 +280,11 @@ class DistZSlab:
         self.esz = [self.sim.component_bytes(c) for c in range(6)]
         self.monitors = []
         self.t = 0
+        # One stream for the slab's kernels, its halo copies and NCCL, so the sends read planes
+        # that are complete and the received planes land before the next launch.  (torch's
+        # default stream would reach the C-ABI as NULL, i.e. the handle's own stream, which
+        # NCCL does not wait for.)
+        self.stream = torch.cuda.Stream(self.device)
 
     def set_coefficients(self, coef12):
         lo, hi = self.plan.loc[self.rank]
@@ -302,7 +307,7 @@ class DistZSlab:
         import torch
         nx, ny, _ = self.shape
         dev = f"cuda:{self.device}"
-        stream = torch.cuda.current_stream(self.device)
+        stream = self.stream
 
         def get_block(k0, nk):
             return _block(self.sim, k0 - self.lo, nk, self.esz, dev, stream)
@@ -313,19 +318,24 @@ class DistZSlab:
         def make_buffer(nk):
             return torch.empty(_block_bytes(self.esz, nk, ny, nx), dtype=torch.uint8, device=dev)
 
-        exchange_dist(self.plan, self.rank, get_block, put_block, make_buffer)
+        with torch.cuda.stream(stream):
+            exchange_dist(self.plan, self.rank, get_block, put_block, make_buffer)
 
     def step(self, T, stream=None):
-        """T steps on the current torch stream (the halo copies and NCCL run on it too)."""
+        """T steps on the slab's stream (kernels, halo copies and NCCL all run on it), ordered
+        after the work queued so far on `stream` (default: the current torch stream), which in
+        turn waits for the steps."""
         import torch
-        st = torch.cuda.current_stream(self.device) if stream is None else stream
+        caller = torch.cuda.current_stream(self.device) if stream is None else stream
+        self.stream.wait_stream(caller)
         done = 0
         while done < int(T):
             b = min(self.plan.halo, int(T) - done)
-            self.sim.step(b, st)
+            self.sim.step(b, self.stream)
             if self.world > 1:
                 self.exchange()
             done += b
+        caller.wait_stream(self.stream)
         self.t += int(T)
 
     def owned_field(self, component):

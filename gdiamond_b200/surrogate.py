@@ -13,13 +13,13 @@ the spectrum is a continuous function of the six numbers rather than a staircase
 
 Excitation and observable: a current sheet on the interior of plane z = 10 driven by the
 Gaussian-modulated sinusoid of the point-source workloads launches a quasi-plane pulse along +z.
-Running DFTs of Ex and Hy on plane z = 86 at 64 frequencies across the source band give the
-transmission spectrum as the z-flux through the plane, Sum Re(Ex conj(Hy)), divided by the same
-flux without the box ("flux"); the coherent normal-incidence amplitude |Sum Ex|^2 / |Sum
-Ex_empty|^2 is available as "amplitude".  (For this x-polarised pulse the Ey Hx* term of the
-flux is second order and is not recorded; the half-cell and half-step offsets of Hy from Ex
-cancel in the ratio to the empty grid.)  The sheet current is transverse (Jx): a z-directed
-current spread uniformly over a z-plane has zero curl and launches no wave along z.
+A Poynting-flux monitor on plane z = 86 at 64 frequencies across the source band
+(fdtd_add_flux_monitor: Re(Ex conj(Hy) - Ey conj(Hx)) summed over the plane, H co-located with
+E in z and phased half a step later) gives the transmission spectrum as that flux divided by
+the same flux without the box ("flux"); the coherent normal-incidence amplitude
+|Sum Ex|^2 / |Sum Ex_empty|^2, from the monitor's Ex DFT, is available as "amplitude".  The
+sheet current is transverse (Jx): a z-directed current spread uniformly over a z-plane has zero
+curl and launches no wave along z.
 
 SpectrumSolver runs designs through the batched FDTD solver (the data generator, the fallback
 and the judge).  Surrogate wraps an ensemble of MLPs 6 -> 256 -> 256 -> 256 -> 64 (GELU, BF16
@@ -80,6 +80,16 @@ def design_eps(p, shape=SHAPE):
     return (1.0 + (e - 1.0) * frac).astype(np.float32).reshape(-1)
 
 
+def bucket(n, group):
+    """Batch size used for n designs: the next power of two (at least 4), at most `group`.
+    Padding a call to a few fixed sizes keeps the number of batches (each created, tuned and
+    graph-captured once) small, so a fallback call of any size costs a predictable time."""
+    b = 4
+    while b < n:
+        b *= 2
+    return min(b, group)
+
+
 class SpectrumSolver:
     """Transmission spectra of designs by batched FDTD (FP32 fields, FP64 DFT sums).
 
@@ -87,7 +97,8 @@ class SpectrumSolver:
 
     Simulations are created once (`group` of them) and reused: each group of designs gets new
     permittivities, a reset, and one persistent batched run of T steps replayed from a CUDA
-    graph.
+    graph.  Groups smaller than `group` are padded to a bucket size (see `bucket`) with copies
+    of their last design, whose results are dropped.
     """
 
     def __init__(self, shape=SHAPE, T=T_STEPS, n_freqs=N_FREQS, group=256, storage="f32",
@@ -106,32 +117,33 @@ class SpectrumSolver:
         nx, ny, _ = self.shape
         self._re = torch.empty((n_freqs, ny, nx), dtype=torch.float64, device=f"cuda:{device}")
         self._im = torch.empty_like(self._re)
-        self._hre = torch.empty_like(self._re)
-        self._him = torch.empty_like(self._re)
+        self._flux = torch.empty((group, n_freqs), dtype=torch.float64, device=f"cuda:{device}")
+        self._ids = {}  # sim -> (flux monitor id, Ex monitor id)
         self.seconds = 0.0  # wall time in measure(): permittivities, batched runs, read-back
 
     def _make(self):
         sim = Simulation(*self.shape, storage=self.storage, device=self.device)
         sim.set_sources([dict(component="Jx", kind=SRC_PLANE_Z, k=self.source_k, wave=self.wave)])
-        sim.add_dft_monitor("Ex", self.monitor_k, self.freqs)
-        sim.add_dft_monitor("Hy", self.monitor_k, self.freqs)
+        fid = sim.add_flux_monitor(self.monitor_k, self.freqs)
+        self._ids[id(sim)] = (fid, sim.flux_monitor_ids(fid)[0])
         return sim
 
     def _measure(self, sims):
-        """[n][n_freqs] complex plane sums of Ex, and real z-fluxes Sum Re(Ex conj(Hy))."""
+        """[n][n_freqs] complex plane sums of Ex, and the z-fluxes of the flux monitors."""
         import torch
         nf = len(self.freqs)
         ex = np.empty((len(sims), nf), np.complex128)
-        flux = np.empty((len(sims), nf), np.float64)
         stream = torch.cuda.current_stream(self.device)
+        exs = torch.empty((len(sims), 2, nf), dtype=torch.float64, device=self._re.device)
         for n, sim in enumerate(sims):
-            sim.get_dft_device(0, self._re.data_ptr(), self._im.data_ptr(), stream)
-            sim.get_dft_device(1, self._hre.data_ptr(), self._him.data_ptr(), stream)
-            r = torch.stack((self._re.sum(dim=(1, 2)), self._im.sum(dim=(1, 2)),
-                             (self._re * self._hre + self._im * self._him).sum(dim=(1, 2))))
-            r = r.cpu().numpy()
-            ex[n] = r[0] + 1j * r[1]
-            flux[n] = r[2]
+            fid, exid = self._ids[id(sim)]
+            sim.get_flux_device(fid, self._flux[n].data_ptr(), stream)
+            sim.get_dft_device(exid, self._re.data_ptr(), self._im.data_ptr(), stream)
+            exs[n, 0] = self._re.sum(dim=(1, 2))
+            exs[n, 1] = self._im.sum(dim=(1, 2))
+        flux = self._flux[:len(sims)].cpu().numpy().copy()
+        e = exs.cpu().numpy()
+        ex[:] = e[:, 0] + 1j * e[:, 1]
         return ex, flux
 
     def empty(self):
@@ -155,24 +167,37 @@ class SpectrumSolver:
         t0 = time.perf_counter()
         for g0 in range(0, len(designs), self.group):
             chunk = designs[g0:g0 + self.group]
-            while len(self.sims) < len(chunk):
+            nb = bucket(len(chunk), self.group)
+            padded = np.concatenate([chunk, np.repeat(chunk[-1:], nb - len(chunk), axis=0)])
+            while len(self.sims) < nb:
                 self.sims.append(self._make())
-            sims = self.sims[:len(chunk)]
-            for sim, p in zip(sims, chunk):
+            sims = self.sims[:nb]
+            for sim, p in zip(sims, padded):
                 sim.set_permittivity(design_eps(p, self.shape), t_pml=self.t_pml)
                 sim.reset()
             for sim in sims:
                 sim.sync()
-            b = self.batches.get(len(chunk))
+            b = self.batches.get(nb)
             if b is None:
-                b = self.batches[len(chunk)] = Batch(sims)
+                b = self.batches[nb] = Batch(sims)
             b.step(self.T)
             for sim in sims:
                 sim.sync()
             e, f = self._measure(sims)
-            ex[g0:g0 + len(chunk)], flux[g0:g0 + len(chunk)] = e, f
+            ex[g0:g0 + len(chunk)], flux[g0:g0 + len(chunk)] = e[:len(chunk)], f[:len(chunk)]
         self.seconds += time.perf_counter() - t0
         return ex, flux
+
+    def warm(self):
+        """Creates, tunes and captures the batch of every bucket size once (one design per
+        call), so later calls of any size run on cached graphs."""
+        b = 4
+        probe = sample_designs(1, seed=12345, shape=self.shape)
+        while True:
+            self.measure(np.repeat(probe, min(b, self.group), axis=0))
+            if b >= self.group:
+                break
+            b *= 2
 
     def to_spectra(self, ex, flux):
         """Spectra [n][n_freqs] of measurements, by the solver's observable."""
@@ -247,3 +272,12 @@ class Surrogate:
 
     def close(self):
         self.net.close()
+
+
+def active_designs(sur, pool, k):
+    """The k designs of `pool` on which the ensemble `sur` disagrees most (active sampling: the
+    solver's runs go where the network is uncertain, the large high-index boxes whose spectra
+    vary fastest)."""
+    mean, sd = sur.predict(pool)
+    order = np.argsort(-Surrogate.disagreement(mean, sd))
+    return np.asarray(pool)[order[:int(k)]]

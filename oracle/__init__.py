@@ -106,6 +106,7 @@ def ref():
         L.gdref_get_fields.restype = C.c_int
         L.gdref_get_fields.argtypes = [C.c_void_p, C.c_int, P(P(C.c_float))]
         L.gdref_max_threads.restype = C.c_int
+        L.gdref_last_printed_seconds.restype = C.c_double
         L.gdref_save_field_png.argtypes = [P(C.c_float), C.c_char_p, C.c_int, C.c_int,
                                            C.c_float]
         _ref = L
@@ -312,6 +313,11 @@ class Reference:
 
     def run_omp_dt(self, blx, bly, blz, blt, T):
         return ref().gdref_run_omp_dt(self.h, blx, bly, blz, blt, T)
+
+    @staticmethod
+    def last_printed_seconds():
+        """The time the reference printed for its own loop in the last run (-1: none)."""
+        return ref().gdref_last_printed_seconds()
 
     def fields(self, variant="seq"):
         v = {"seq": 0, "omp": 1, "omp_dt": 2}[variant]

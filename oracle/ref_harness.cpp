@@ -64,6 +64,23 @@ double seconds_since(std::chrono::high_resolution_clock::time_point t0) {
   return std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t0).count();
 }
 
+// The time the reference prints for its own loop ("... runtime: <s>s") during the last run.
+double g_printed = -1.0;
+
+// Runs f with std::cout captured, keeps the printed runtime, and echoes the text.
+template <typename F>
+void capture_printed(F f) {
+  std::ostringstream cap;
+  std::streambuf* old = std::cout.rdbuf(cap.rdbuf());
+  f();
+  std::cout.rdbuf(old);
+  const std::string text = cap.str();
+  g_printed = -1.0;
+  const size_t at = text.find("runtime: ");
+  if (at != std::string::npos) g_printed = std::strtod(text.c_str() + at + 9, nullptr);
+  std::cout << text << std::flush;
+}
+
 }  // namespace
 
 extern "C" {
@@ -98,7 +115,7 @@ void gdref_params(void* h, float* out7) {
 // the time loop and the copy-out included).
 double gdref_run_seq(void* h, size_t T) {
   auto t0 = std::chrono::high_resolution_clock::now();
-  static_cast<gDiamond*>(h)->update_FDTD_seq(T);
+  capture_printed([&] { static_cast<gDiamond*>(h)->update_FDTD_seq(T); });
   return seconds_since(t0);
 }
 
@@ -106,7 +123,7 @@ double gdref_run_omp(void* h, size_t T) {
   gDiamond* g = static_cast<gDiamond*>(h);
   resize_variant(g, 1);
   auto t0 = std::chrono::high_resolution_clock::now();
-  g->update_FDTD_omp(T);
+  capture_printed([&] { g->update_FDTD_omp(T); });
   return seconds_since(t0);
 }
 
@@ -114,7 +131,7 @@ double gdref_run_omp_dt(void* h, size_t blx, size_t bly, size_t blz, size_t blt,
   gDiamond* g = static_cast<gDiamond*>(h);
   resize_variant(g, 2);
   auto t0 = std::chrono::high_resolution_clock::now();
-  g->update_FDTD_omp_dt(blx, bly, blz, blt, T);
+  capture_printed([&] { g->update_FDTD_omp_dt(blx, bly, blz, blt, T); });
   return seconds_since(t0);
 }
 
@@ -132,6 +149,10 @@ int gdref_get_fields(void* h, int variant, float* const* out6) {
 }
 
 int gdref_max_threads(void) { return omp_get_max_threads(); }
+
+// The runtime the reference printed for its own time loop in the last gdref_run_* call (its
+// chrono clock around the loop only), or -1 when it printed none.
+double gdref_last_printed_seconds(void) { return g_printed; }
 
 // The reference's field-slice PNG writer (blue-white-red map clipped to +-vmax).
 void gdref_save_field_png(const float* u, const char* filename, int nx, int ny, float vmax) {

@@ -98,3 +98,11 @@ def test_null_handle_calls_return_invalid_arg():
     assert L.fdtd_step(None, 1, None) == 1
     assert L.fdtd_sync(None) == 1
     assert L.fdtd_destroy(None) == 1
+
+
+def test_surrogate_fallback_bucket_sizes():
+    """Fallback calls are padded to a few batch sizes (powers of two from 4, at most the group)."""
+    from gdiamond_b200 import surrogate as S
+    assert [S.bucket(n, 256) for n in (1, 3, 4, 5, 9, 100, 256, 300)] == \
+        [4, 4, 4, 8, 16, 128, 256, 256]
+    assert S.bucket(7, 6) == 6
