@@ -344,6 +344,8 @@ def run_ours(args):
                         tile_rows=args.rows, z_chunks=args.zchunks, min_blocks=args.min_blocks)
     sim.set_coefficients(coefs)
     sim.set_fast_path(not args.no_fast_path)
+    if args.cpml:
+        sim.set_cpml(thickness=args.cpml)  # per-step E/H kernels with CPML layers
     sim.set_sources(src)
     mid = sim.add_dft_monitor("Ez", nz // 2, freqs, scale=1.0)
     stream = torch.cuda.Stream()
@@ -474,11 +476,15 @@ def run_ours(args):
                    "l2": "inputs (1.2 GB of fields) larger than L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
+                     "dram_gbs": traffic / (launch_ms / 1e3) / 1e9 if traffic else None,
+                     "dram_frac": traffic / (launch_ms / 1e3) / 1e9 / hbm if traffic else None,
+                     "dram_bytes_per_cell_update": traffic / cells_per_launch if traffic else None,
                      "note": f"achieved = {B_ALG} B/cell-update x {cells_per_launch} cell-updates "
                              f"per launch / mean launch time {launch_ms:.4f} ms (step time / "
                              f"{launches_per_step} tiled launches; the step's "
                              f"{cfg['dft_folds']} DFT folds included); peak {kind}; "
-                             f"temporal tiling lets frac exceed 1"},
+                             f"temporal tiling lets frac exceed 1; dram_frac = the measured "
+                             f"DRAM bytes of one launch (ncu, profiles/) over the same time"},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": (launches_per_step + cfg["dft_folds"]) * args.steps,
@@ -495,7 +501,7 @@ def run_zslab(args, rank, world, local, dist, barrier, max_over_ranks):
     the whole grid, 8-frequency DFT of Ez on its middle plane, 1000 steps): weak scaling.  Each
     rank holds its owned planes plus BLT halo planes below and BLT + 1 above; after every
     tiled launch of BLT steps the ranks exchange (2 BLT + 1) planes of all six components per
-    interior face with NCCL send/receive into their own device buffers (no multicast, no peer
+    interior face with NCCL send/receive into their own device buffers (plain copies, no peer
     loads).  Timed like the single-GPU line: CUDA events on the launching stream, barriers on
     both sides, max over ranks; `value` counts the cells of the whole grid."""
     import torch
@@ -1068,6 +1074,9 @@ def main():
     ap.add_argument("--parallelism", default="zslab", choices=["zslab", "replicas"],
                     help="N > 1: one grid split into z-slabs over the GPUs (halo exchange), or "
                          "an independent replica per GPU")
+    ap.add_argument("--cpml", type=int, default=0,
+                    help="CPML layers of this many cells on every face (the per-step E/H "
+                         "kernels instead of the tiled kernel)")
     ap.add_argument("--no-fast-path", action="store_true",
                     help="force the general per-cell path of the x-pair kernels")
     ap.add_argument("--workload", default="plain",

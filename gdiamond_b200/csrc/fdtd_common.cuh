@@ -212,7 +212,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   }
 }
 
-// Tiled 3-D TMA load global -> shared (no multicast), completing on `bar`.
+// Tiled 3-D TMA load global -> this CTA's shared memory, completing on `bar`.
 __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, uint64_t* bar, int x,
                                             int y, int z) {
   asm volatile(

@@ -6,7 +6,7 @@
 //
 //  * A CTA owns a 32 x ROWS column of the x-y plane (one warp per row, one cell per thread) and
 //    marches along z.  Each z-plane of the six fields and of the uint16 material map is staged
-//    into shared memory by TMA (cp.async.bulk.tensor, no multicast) through a 3-stage mbarrier
+//    into shared memory by TMA (cp.async.bulk.tensor into this CTA's own shared memory) through a 3-stage mbarrier
 //    pipeline, so HBM reads run ahead of the arithmetic.
 //  * BLT time levels run as a wavefront in (z, t): when plane p arrives, level s computes
 //    E^s at plane p-s+1 and H^s at plane p-s.  Neighbours along z are the thread's own values

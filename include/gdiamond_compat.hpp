@@ -134,6 +134,7 @@ class gDiamond {
                      (int64_t)(_Nz / 2)};
     run_gpu_sources(num_timesteps, &s, 1, w, GPU, FDTD_KERNEL_AUTO, true,
                     50.0 / (double)num_timesteps);
+    _fig_wave = std::move(w);
   }
 
   // ------------------------------------------------------------------ checks
@@ -149,6 +150,8 @@ class gDiamond {
   const std::vector<double>& dft_real() const { return _dft_re; }
   const std::vector<double>& dft_imag() const { return _dft_im; }
   const std::vector<double>& dft_freqs() const { return _freqs; }
+  // The Jx waveform of the last update_FDTD_gpu_figures call (sample t used at step t).
+  const std::vector<float>& figures_wave() const { return _fig_wave; }
   size_t source_idx() const { return _source_idx; }
   size_t Nx() const { return _Nx; }
   size_t Ny() const { return _Ny; }
@@ -415,6 +418,7 @@ class gDiamond {
   std::vector<float> _res[5][6];
   mutable const float* _cptr[12] = {};
   std::vector<double> _freqs, _dft_re, _dft_im;
+  std::vector<float> _fig_wave;
   fdtd_handle* _h = nullptr;
   int _h_kernel = -1;
   int32_t _mon_id = -1;

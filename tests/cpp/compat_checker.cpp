@@ -6,7 +6,9 @@
 //                                                 optional raw dump of seq fields
 //   compat_checker gpu Nx Ny Nz T [dump_prefix]   seq vs gpu_2D, 3D-fix vs mix-mapping ver3,
 //                                                 ver3 vs the vectorized 3D-fix alias,
-//                                                 the figures path (Jx + Ex DFT)
+//                                                 the figures path (Jx + Ex DFT); with
+//                                                 dump_prefix, its waveform, frequencies,
+//                                                 DFT sums and coefficients as raw files
 // Prints one JSON object; exit code 0 when every check holds.
 #include <cstdio>
 #include <cstring>
@@ -14,6 +16,12 @@
 #include <string>
 
 #include "gdiamond_compat.hpp"
+
+template <class T>
+static void dump(const std::string& path, const std::vector<T>& v) {
+  std::ofstream f(path, std::ios::binary);
+  f.write(reinterpret_cast<const char*>(v.data()), v.size() * sizeof(T));
+}
 
 static double l2(const std::vector<float>& v) {
   double s = 0;
@@ -68,6 +76,14 @@ int main(int argc, char** argv) {
     double dmax = 0;
     for (double v : exp.dft_real()) dmax = std::max(dmax, std::fabs(v));
     const bool figs = exp.dft_freqs().size() == 26 && dmax > 0 && std::isfinite(dmax);
+    if (argc > 6) {
+      const std::string pre = argv[6];
+      dump(pre + "fig_wave.bin", exp.figures_wave());
+      dump(pre + "fig_freqs.bin", exp.dft_freqs());
+      dump(pre + "fig_re.bin", exp.dft_real());
+      dump(pre + "fig_im.bin", exp.dft_imag());
+      for (int a = 0; a < 12; ++a) dump(pre + "coef" + std::to_string(a) + ".bin", exp.coefficient(a));
+    }
     ok = ok && g2 && g3 && gv && figs;
     std::printf(", \"gpu_2D_matches_seq\": %s, \"ver3_matches_3D_fix\": %s, "
                 "\"vectorized_matches_ver3\": %s, \"figures_nf\": %zu, \"figures_dft_max\": %.17g",

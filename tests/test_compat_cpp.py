@@ -49,9 +49,22 @@ def test_cpp_seq_matches_golden_and_omp(checker, tmp_path):
 
 
 @pytest.mark.gpu
-def test_cpp_gpu_paths_match_reference_checks(checker):
-    rc, res = run(checker, "gpu", 64, 56, 48, 90)
+def test_cpp_gpu_paths_match_reference_checks(checker, tmp_path):
+    shape, T = (64, 56, 48), 90
+    rc, res = run(checker, "gpu", *shape, T, str(tmp_path / "g_"))
     assert res["gpu_2D_matches_seq"] and res["ver3_matches_3D_fix"]
     assert res["vectorized_matches_ver3"]
     assert res["figures_nf"] == 26 and res["figures_dft_max"] > 0
     assert rc == 0
+    # the figures path's Ex DFT (Jx point source, plane Nz/2) against the oracle's FP64 DFT,
+    # bit for bit, from the waveform, frequencies and coefficients the class used
+    import oracle
+    nx, ny, nz = shape
+    rd = lambda name, dt: np.fromfile(tmp_path / f"g_{name}.bin", dtype=dt)
+    wave, freqs = rd("fig_wave", np.float32), rd("fig_freqs", np.float64)
+    coefs = [rd(f"coef{a}", np.float32) for a in range(12)]
+    mon = oracle.Monitor("Ex", nz // 2, freqs, scale=50.0 / T)
+    oracle.run(shape, coefs, T, sources=[oracle.Source("Jx", wave, i=nx // 2, j=ny // 2, k=nz // 2)],
+               monitors=[mon], dt=float(np.float32(0.05)))
+    re, im = rd("fig_re", np.float64), rd("fig_im", np.float64)
+    assert np.array_equal(re, mon.re.reshape(-1)) and np.array_equal(im, mon.im.reshape(-1))
