@@ -74,26 +74,18 @@ __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 
-// Paired FP32 arithmetic (sm_100 `.f32x2`): one instruction for both cells of an x-pair, each
-// half rounded to nearest even with subnormals kept, i.e. __fadd_rn / __fsub_rn applied to .x
-// and .y (checked on the B200 against the scalar forms, subnormal and signed-zero operands
-// included).  There is deliberately no paired multiply: a paired multiply followed by a paired
-// add is evaluated as one paired fused multiply-add (even when both are written with an
-// explicit .rn), whose single rounding differs from the reference's separately rounded
-// product and sum; scale2 multiplies each half on its own (__fmul_rn is never fused).
-#define GD_F32X2_OP(NAME, OP)                                                                 \
-  __device__ __forceinline__ float2 NAME(float2 a, float2 b) {                                \
-    float2 d;                                                                                 \
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\t"                                                     \
-        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t" OP                              \
-        " rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"                                           \
-        : "=f"(d.x), "=f"(d.y)                                                                \
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                            \
-    return d;                                                                                 \
-  }
-GD_F32X2_OP(add2, "add.rn.f32x2")
-GD_F32X2_OP(sub2, "sub.rn.f32x2")
-#undef GD_F32X2_OP
+// Paired FP32 arithmetic (sm_100 `.f32x2`, CUDA's __fadd2_rn): one instruction for both cells
+// of an x-pair, each half rounded to nearest even with subnormals kept, i.e. __fadd_rn applied
+// to .x and .y; a - b is a + (-b), which IEEE arithmetic rounds identically (negation is exact).
+// The fast-path tests compare the paired lean update with the scalar general update bit for bit.
+// There is deliberately no paired multiply: a paired multiply followed by a paired add was
+// evaluated as one paired fused multiply-add (even when both were written with an explicit .rn),
+// whose single rounding differs from the reference's separately rounded product and sum;
+// scale2 multiplies each half on its own (__fmul_rn is never fused).
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  return __fadd2_rn(a, make_float2(-b.x, -b.y));
+}
 __device__ __forceinline__ float2 scale2(float c, float2 v) {
   return make_float2(__fmul_rn(c, v.x), __fmul_rn(c, v.y));
 }
