@@ -885,7 +885,7 @@ def run_surrogate(args):
     import torch
     from gdiamond_b200 import surrogate as S
     T = args.timesteps if args.timesteps != T_STEPS else S.T_STEPS
-    sol = S.SpectrumSolver(T=T, group=256, observable=args.observable)
+    sol = S.SpectrumSolver(T=T, group=256, observable=args.observable, boundary=args.boundary)
     out = {}
     if args.surrogate_data:
         d = np.load(args.surrogate_data)
@@ -977,7 +977,8 @@ def run_surrogate(args):
     pk = json.load(open(pk_path)) if os.path.exists(pk_path) else {"bf16_tflops": 1590.0}
     out["inference_1M"] = {"designs_per_s": n_inf / sec, "tflops": flop / sec / 1e12,
                            "frac_of_bf16_peak": flop / sec / 1e12 / pk["bf16_tflops"]}
-    out["surrogate"] = {"observable": args.observable, "train_seconds": t_fit,
+    out["surrogate"] = {"observable": args.observable, "boundary": args.boundary,
+                        "flux_plane": sol.monitor_k, "train_seconds": t_fit,
                         "bucket_warmup_seconds": t_warm,
                         "epochs": args.epochs, "batch": args.mlp_batch,
                         "final_loss_per_member": [float(v) for v in losses[-1]],
@@ -992,7 +993,8 @@ def run_surrogate(args):
     sol.close()
     line = {"metric": "designs/s (surrogate with FDTD fallback vs batched solver) at stated "
                       "held-out spectral error",
-            "workload": f"box designs in 96^3, T={T}, 64-freq transmission ({args.observable}), "
+            "workload": f"box designs in 96^3, T={T}, 64-freq transmission ({args.observable}, "
+                        f"{'CPML' if args.boundary == 'cpml' else 'graded pseudo-PML'}), "
                         f"{len(train)} train + {len(test)} held-out",
             "results": out, "data": "synthetic (seeded designs)"}
     print(json.dumps(line))
@@ -1096,6 +1098,8 @@ def main():
                          "disagreement of a first ensemble (active sampling)")
     ap.add_argument("--epochs", type=int, default=200, help="surrogate: training epochs")
     ap.add_argument("--mlp-batch", type=int, default=64, help="surrogate: minibatch rows")
+    ap.add_argument("--boundary", default="pml", choices=["pml", "cpml"],
+                    help="surrogate: the reference's graded pseudo-PML or CPML layers")
     ap.add_argument("--observable", default="flux", choices=["flux", "amplitude"],
                     help="surrogate: transmission observable")
     ap.add_argument("--surrogate-data", default="",

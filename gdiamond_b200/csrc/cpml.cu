@@ -13,7 +13,11 @@
 // and likewise for the other five components.  Profiles along each axis are tabulated at the E
 // positions (integer n) and the H positions (n + 1/2).  Outside every layer a component's update
 // is the reference's formula, operation for operation, so the interior stays bit-identical to
-// the non-PML solver; psi is stored only in the slabs of its axis (2 (L + 1) positions).
+// the non-PML solver; psi is stored only in the slabs of its axis (2L + 1 positions).
+//
+// One grid: cpml_e / cpml_h per step, monitors accumulated per step.  A batch of grids:
+// cpml_e_batch / cpml_h_batch cover every grid in one launch each (blockIdx.z = grid * max_nz
+// + k, arguments from a device array) and stage the monitor values for the deferred DFT.
 #include "fdtd_kernels.cuh"
 
 namespace fdtd {
@@ -24,28 +28,28 @@ struct CoefRefs {
   const float* c[12];  // pitched per-cell arrays (or null with a material map)
 };
 
-__device__ __forceinline__ void e_coefs(const CoefRefs& A, const uint16_t* mat, const Material* tab,
-                                        long long idx, float* ca, float* cb) {
+__device__ __forceinline__ void e_coefs(const float* const* A, const uint16_t* mat,
+                                        const Material* tab, long long idx, float* ca, float* cb) {
   if (mat) {
     const Material m = tab[mat[idx]];
     ca[0] = m.a.x; cb[0] = m.a.y; ca[1] = m.a.z; cb[1] = m.a.w; ca[2] = m.b.x; cb[2] = m.b.y;
   } else {
     for (int c = 0; c < 3; ++c) {
-      ca[c] = A.c[c][idx];
-      cb[c] = A.c[3 + c][idx];
+      ca[c] = A[c][idx];
+      cb[c] = A[3 + c][idx];
     }
   }
 }
 
-__device__ __forceinline__ void h_coefs(const CoefRefs& A, const uint16_t* mat, const Material* tab,
-                                        long long idx, float* da, float* db) {
+__device__ __forceinline__ void h_coefs(const float* const* A, const uint16_t* mat,
+                                        const Material* tab, long long idx, float* da, float* db) {
   if (mat) {
     const Material m = tab[mat[idx]];
     da[0] = m.b.z; db[0] = m.b.w; da[1] = m.c.x; db[1] = m.c.y; da[2] = m.c.z; db[2] = m.c.w;
   } else {
     for (int c = 0; c < 3; ++c) {
-      da[c] = A.c[6 + c][idx];
-      db[c] = A.c[9 + c][idx];
+      da[c] = A[6 + c][idx];
+      db[c] = A[9 + c][idx];
     }
   }
 }
@@ -75,12 +79,15 @@ __device__ __forceinline__ bool src_sum(const Sources& S, int comp, int i, int j
   return source_value(S, comp, i, j, k, t, v);
 }
 
-// grid (ceil(nx/32), ceil(ny/4), nz), block (32, 4); interior cells only, in place.
-__global__ void __launch_bounds__(128) cpml_e(Grid g, FieldPtrs F, CoefRefs A, const uint16_t* mat,
-                                              const Material* tab, Sources S, long long t,
-                                              float dx, CpmlDev P) {
-  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, k = blockIdx.z;
-  if (i < 1 || i > g.nx - 2 || j < 1 || j > g.ny - 2 || k < 1 || k > g.nz - 2) return;
+__device__ __forceinline__ bool interior(const Grid& g, int i, int j, int k) {
+  return i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2;
+}
+
+// E update of interior cell (i, j, k) at step t, in place.
+__device__ __forceinline__ void e_cell(const Grid& g, const FieldPtrs& F, const float* const* A,
+                                       const uint16_t* mat, const Material* tab,
+                                       const Sources& S, long long t, float dx, const CpmlDev& P,
+                                       int i, int j, int k) {
   const long long sy = g.pitch, sz = g.plane, idx = i + j * sy + k * sz;
   float* const* f = F.f;
   const float hx = f[3][idx], hy = f[4][idx], hz = f[5][idx];
@@ -118,11 +125,11 @@ __global__ void __launch_bounds__(128) cpml_e(Grid g, FieldPtrs F, CoefRefs A, c
   f[2][idx] = yee(ca[2], f[2][idx], cb[2], cz);
 }
 
-__global__ void __launch_bounds__(128) cpml_h(Grid g, FieldPtrs F, CoefRefs A, const uint16_t* mat,
-                                              const Material* tab, Sources S, long long t,
-                                              float dx, CpmlDev P) {
-  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, k = blockIdx.z;
-  if (i < 1 || i > g.nx - 2 || j < 1 || j > g.ny - 2 || k < 1 || k > g.nz - 2) return;
+// H update of interior cell (i, j, k) at step t, in place (after every E update of the step).
+__device__ __forceinline__ void h_cell(const Grid& g, const FieldPtrs& F, const float* const* A,
+                                       const uint16_t* mat, const Material* tab,
+                                       const Sources& S, long long t, float dx, const CpmlDev& P,
+                                       int i, int j, int k) {
   const long long sy = g.pitch, sz = g.plane, idx = i + j * sy + k * sz;
   float* const* f = F.f;
   const float ex = f[0][idx], ey = f[1][idx], ez = f[2][idx];
@@ -160,7 +167,75 @@ __global__ void __launch_bounds__(128) cpml_h(Grid g, FieldPtrs F, CoefRefs A, c
   f[5][idx] = yee(da[2], f[5][idx], db[2], cz);
 }
 
+// One grid: grid (ceil(nx/32), ceil(ny/4), nz), block (32, 4); interior cells only.
+__global__ void __launch_bounds__(128) cpml_e(Grid g, FieldPtrs F, CoefRefs A, const uint16_t* mat,
+                                              const Material* tab, Sources S, long long t,
+                                              float dx, CpmlDev P) {
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, k = blockIdx.z;
+  if (interior(g, i, j, k)) e_cell(g, F, A.c, mat, tab, S, t, dx, P, i, j, k);
+}
+
+__global__ void __launch_bounds__(128) cpml_h(Grid g, FieldPtrs F, CoefRefs A, const uint16_t* mat,
+                                              const Material* tab, Sources S, long long t,
+                                              float dx, CpmlDev P) {
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, k = blockIdx.z;
+  if (interior(g, i, j, k)) h_cell(g, F, A.c, mat, tab, S, t, dx, P, i, j, k);
+}
+
+// Monitor values of cell (i, j) of plane k at step t into the staging rings: the E monitors
+// after the E update (e_comps), the H monitors after the H update.  Face cells, which the update
+// leaves unchanged, are staged too: the fold reads every cell of the plane.
+__device__ __forceinline__ void stage_cell(const CpmlSim& s, long long t, int i, int j, int k,
+                                           bool e_comps) {
+  for (int n = 0; n < s.M.n; ++n) {
+    const MonitorDev& m = s.M.m[n];
+    if ((m.comp < 3) != e_comps || m.k != k) continue;
+    const long long idx = i + (long long)j * s.g.pitch + (long long)k * s.g.plane;
+    dft_record(m, t, i, j, s.g, s.F.f[m.comp][idx]);
+  }
+}
+
+// A batch: blockIdx.z = grid * max_nz + k over the grids' argument array.
+__global__ void __launch_bounds__(128) cpml_e_batch(const CpmlSim* sims, int max_nz,
+                                                    long long t_offset) {
+  const CpmlSim& s = sims[blockIdx.z / max_nz];
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
+  const int k = (int)(blockIdx.z % max_nz);
+  if (i >= s.g.nx || j >= s.g.ny || k >= s.g.nz) return;
+  const long long t = s.t0 + t_offset;
+  if (interior(s.g, i, j, k)) e_cell(s.g, s.F, s.coef, s.mat, s.tab, s.S, t, s.dx, s.P, i, j, k);
+  if (s.M.n) stage_cell(s, t, i, j, k, true);
+}
+
+__global__ void __launch_bounds__(128) cpml_h_batch(const CpmlSim* sims, int max_nz,
+                                                    long long t_offset) {
+  const CpmlSim& s = sims[blockIdx.z / max_nz];
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
+  const int k = (int)(blockIdx.z % max_nz);
+  if (i >= s.g.nx || j >= s.g.ny || k >= s.g.nz) return;
+  const long long t = s.t0 + t_offset;
+  if (interior(s.g, i, j, k)) h_cell(s.g, s.F, s.coef, s.mat, s.tab, s.S, t, s.dx, s.P, i, j, k);
+  if (s.M.n) stage_cell(s, t, i, j, k, false);
+}
+
 }  // namespace
+
+cudaError_t launch_cpml_batch_step(const CpmlSim* sims, int nsims, int max_nx, int max_ny,
+                                   int max_nz, long long t_offset, cudaStream_t st) {
+  if (nsims <= 0) return cudaSuccess;
+  if (max_nz <= 0 || max_nz > 65535) return cudaErrorInvalidValue;
+  // grids per launch pair: blockIdx.z stays within its 65535 limit (grids are independent, so
+  // each group's E launch before its H launch is all the order a step needs)
+  const int per = 65535 / max_nz;
+  const dim3 blk(32, 4);
+  for (int g0 = 0; g0 < nsims; g0 += per) {
+    const int n = nsims - g0 < per ? nsims - g0 : per;
+    const dim3 grd((max_nx + 31) / 32, (max_ny + 3) / 4, (unsigned)(n * max_nz));
+    cpml_e_batch<<<grd, blk, 0, st>>>(sims + g0, max_nz, t_offset);
+    cpml_h_batch<<<grd, blk, 0, st>>>(sims + g0, max_nz, t_offset);
+  }
+  return cudaGetLastError();
+}
 
 cudaError_t launch_cpml_step(const Grid& g, const FieldPtrs& F, const float* const* coef,
                              const uint16_t* mat, const Material* tab, const Sources& S,

@@ -66,10 +66,12 @@ __global__ void __launch_bounds__(kFoldThreads) dft_fold(const __grid_constant__
 }
 
 // A batch: blockIdx.z is the grid; its arguments (monitors, step counter t0 at the start of the
-// batch step) are the ones the batched kernel reads.  The window starts t_offset steps later.
-__global__ void __launch_bounds__(kFoldThreads) dft_fold_batch(const TiledArgs* grids,
+// batch step) are the ones the batched kernel reads (TiledArgs, or CpmlSim for CPML batches).
+// The window starts t_offset steps later.
+template <class Args>
+__global__ void __launch_bounds__(kFoldThreads) dft_fold_batch(const Args* grids,
                                                                long long t_offset, int n) {
-  const TiledArgs& a = grids[blockIdx.z];
+  const Args& a = grids[blockIdx.z];
   for (int k = 0; k < a.M.n; ++k) fold_monitor(a.M.m[k], a.g, a.t0 + t_offset, n);
 }
 
@@ -94,7 +96,17 @@ cudaError_t launch_dft_fold_batch(const TiledArgs* grids, int ngrids, long long 
                                   int max_nf, long long t_offset, int n, cudaStream_t st) {
   if (ngrids <= 0 || max_nf <= 0 || n <= 0) return cudaSuccess;
   if (n > kDftSlots || t_offset < 0 || ngrids > 65535) return cudaErrorInvalidValue;
-  dft_fold_batch<<<fold_grid(max_np, max_nf, ngrids), kFoldThreads, 0, st>>>(grids, t_offset, n);
+  dft_fold_batch<TiledArgs>
+      <<<fold_grid(max_np, max_nf, ngrids), kFoldThreads, 0, st>>>(grids, t_offset, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dft_fold_cpml_batch(const CpmlSim* sims, int nsims, long long max_np,
+                                       int max_nf, long long t_offset, int n, cudaStream_t st) {
+  if (nsims <= 0 || max_nf <= 0 || n <= 0) return cudaSuccess;
+  if (n > kDftSlots || t_offset < 0 || nsims > 65535) return cudaErrorInvalidValue;
+  dft_fold_batch<CpmlSim>
+      <<<fold_grid(max_np, max_nf, nsims), kFoldThreads, 0, st>>>(sims, t_offset, n);
   return cudaGetLastError();
 }
 

@@ -1520,6 +1520,9 @@ struct fdtd_batch {
   std::vector<long long> gkey;
   int gfolds = 0;  // DFT fold launches in the captured graph
   int last_launches = 0, last_graph = 0, last_folds = 0;
+  // CPML batches (every simulation has CPML layers): per-grid arguments of the per-step kernels
+  fdtd::CpmlSim* d_cpml = nullptr;
+  fdtd::CpmlSim* h_cpml = nullptr;  // pinned staging, copied to d_cpml at the head of a step
   std::string err;
 };
 
@@ -1723,6 +1726,112 @@ fdtd_status stream_after(fdtd_batch* b, cudaStream_t waiter, cudaStream_t on) {
   return FDTD_OK;
 }
 
+// A batch whose simulations have CPML layers: per step one E and one H launch over every grid
+// (in place, FP32), monitor values staged in the rings and folded before a ring would wrap and
+// at the end, as in the tiled batches.  With use_graph the T steps are captured once and
+// replayed; the argument table is refreshed by the copy at the head of the sequence, so the
+// graph only depends on T and the batch's extents.
+fdtd_status batch_step_cpml(fdtd_batch* b, int64_t T, int32_t use_graph, cudaStream_t st) {
+  const int n = (int)b->sims.size();
+  if (!b->h_cpml) {
+    BCUDA(b, cudaMalloc(&b->d_cpml, n * sizeof(fdtd::CpmlSim)));
+    BCUDA(b, cudaMallocHost(&b->h_cpml, n * sizeof(fdtd::CpmlSim)));
+  }
+  int max_nx = 0, max_ny = 0, max_nz = 0, max_nf = 0;
+  long long max_np = 0;
+  for (int i = 0; i < n; ++i) {
+    const fdtd_handle* h = b->sims[i];
+    if (h->storage != FDTD_STORE_F32)
+      return bfail(b, FDTD_ERR_UNSUPPORTED, "CPML layers need FP32 field storage");
+    fdtd::CpmlSim& a = b->h_cpml[i];
+    a = fdtd::CpmlSim{};
+    a.g = h->g;
+    for (int c = 0; c < 6; ++c) a.F.f[c] = h->F[h->cur][c];
+    a.mat = h->mat;  // batches hold material maps only
+    a.tab = h->table;
+    a.S = make_sources(h);
+    a.M = make_monitors(h);
+    a.P = h->cpml_dev;
+    a.t0 = h->t;
+    a.dx = h->desc.dx;
+    max_nx = std::max(max_nx, h->g.nx);
+    max_ny = std::max(max_ny, h->g.ny);
+    max_nz = std::max(max_nz, h->g.nz);
+    for (int m = 0; m < h->nmon; ++m) {
+      max_np = std::max<long long>(max_np, (long long)h->g.nx * h->g.ny);
+      max_nf = std::max(max_nf, h->mon[m].nf);
+    }
+  }
+  int folds = 0;
+  auto record = [&](cudaStream_t rs) -> fdtd_status {
+    BCUDA(b, cudaMemcpyAsync(b->d_cpml, b->h_cpml, n * sizeof(fdtd::CpmlSim),
+                             cudaMemcpyHostToDevice, rs));
+    long long folded = 0;
+    folds = 0;
+    for (long long q = 0; q < T; ++q) {
+      if (max_nf > 0 && q + 1 - folded > fdtd::kDftSlots) {
+        BCUDA(b, fdtd::launch_dft_fold_cpml_batch(b->d_cpml, n, max_np, max_nf, folded,
+                                                  (int)(q - folded), rs));
+        ++folds;
+        folded = q;
+      }
+      BCUDA(b, fdtd::launch_cpml_batch_step(b->d_cpml, n, max_nx, max_ny, max_nz, q, rs));
+    }
+    if (max_nf > 0 && T > folded) {
+      BCUDA(b, fdtd::launch_dft_fold_cpml_batch(b->d_cpml, n, max_np, max_nf, folded,
+                                                (int)(T - folded), rs));
+      ++folds;
+    }
+    return FDTD_OK;
+  };
+  b->last_graph = 0;
+  if (use_graph) {
+    const std::vector<long long> key = {-1, T, n, max_nx, max_ny, max_nz, max_np, max_nf};
+    if (!b->gexec || key != b->gkey) {
+      if (b->gexec) {
+        cudaGraphExecDestroy(b->gexec);
+        b->gexec = nullptr;
+      }
+      cudaGraph_t graph;
+      BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
+      fdtd_status r = record(b->stream);
+      cudaError_t ce = cudaStreamEndCapture(b->stream, &graph);
+      if (r != FDTD_OK) return r;
+      if (ce != cudaSuccess) return bfail(b, FDTD_ERR_CUDA, "graph capture failed: %s",
+                                          cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&b->gexec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return bfail(b, FDTD_ERR_CUDA, "graph instantiation failed: %s",
+                                          cudaGetErrorString(ce));
+      b->gkey = key;
+      b->gfolds = folds;
+    } else {
+      b->last_graph = 1;
+      folds = b->gfolds;
+    }
+    BCUDA(b, cudaGraphLaunch(b->gexec, st));
+  } else {
+    fdtd_status r = record(st);
+    if (r != FDTD_OK) return r;
+  }
+  if (!b->args_read) BCUDA(b, cudaEventCreateWithFlags(&b->args_read, cudaEventDisableTiming));
+  BCUDA(b, cudaEventRecord(b->args_read, st));
+  b->args_pending = true;
+  const int per = 65535 / std::max(max_nz, 1);
+  const int launches = (int)(2 * T * ((n + per - 1) / per));
+  for (fdtd_handle* h : b->sims) {
+    h->t += T;
+    h->last_kernel = 6;  // the per-step CPML kernels
+    h->last_launches = launches;
+    h->last_folds = folds;
+    fdtd_status r = stream_after(b, h->stream, st);
+    if (r != FDTD_OK) return r;
+  }
+  b->last_launches = launches;
+  b->last_folds = folds;
+  return FDTD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1744,6 +1853,9 @@ fdtd_status fdtd_batch_create(fdtd_handle* const* sims, int32_t n, fdtd_batch** 
     if (h->coef_mode != kCoefMaterial)
       return bfail(nullptr, FDTD_ERR_UNSUPPORTED,
                    "simulation %d has no material map (coefficients not set or too many)", i);
+    if (h->cpml_on != sims[0]->cpml_on)
+      return bfail(nullptr, FDTD_ERR_INVALID_ARG,
+                   "simulations must all have CPML layers or all have none");
   }
   fdtd_batch* b = new fdtd_batch();
   b->sims.assign(sims, sims + n);
@@ -1771,6 +1883,8 @@ fdtd_status fdtd_batch_destroy(fdtd_batch* b) {
   cudaFree(b->d_counters);
   cudaFree(b->d_args);
   if (b->h_args) cudaFreeHost(b->h_args);
+  cudaFree(b->d_cpml);
+  if (b->h_cpml) cudaFreeHost(b->h_cpml);
   if (b->args_read) cudaEventDestroy(b->args_read);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -1791,6 +1905,11 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int64_t T, int32_t use_graph, void* s
     if ((s = ensure_tables(h, h->t + T)) != FDTD_OK) return bfail(b, s, "%s", h->err.c_str());
     if ((s = stream_after(b, st, h->stream)) != FDTD_OK) return s;
   }
+  for (const fdtd_handle* h : b->sims)  // layers may have been set after the batch was made
+    if (h->cpml_on != b->sims[0]->cpml_on)
+      return bfail(b, FDTD_ERR_INVALID_ARG,
+                   "simulations must all have CPML layers or all have none");
+  if (b->sims[0]->cpml_on) return batch_step_cpml(b, T, use_graph, st);
   if (!b->cfg_ready && (s = batch_autotune(b, st)) != FDTD_OK) return s;
   const fdtd::TiledConfig c = b->cfg;
   const long long nfull = T / c.blt;

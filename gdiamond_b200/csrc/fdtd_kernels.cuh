@@ -45,6 +45,30 @@ cudaError_t launch_cpml_step(const Grid& g, const FieldPtrs& F, const float* con
                              const Monitors& M, const CpmlDev& P, long long t, float dx,
                              cudaStream_t st, int* launches);
 
+// One grid of a batch of CPML simulations (device-resident array, built by the host per batch
+// step): fields are updated in place; monitor values go to the staging rings (dft_record) and
+// are folded by launch_dft_fold_cpml_batch.  t0 = the grid's step counter at the start of the
+// batch step.
+struct CpmlSim {
+  Grid g;
+  FieldPtrs F;
+  const float* coef[12];  // pitched per-cell arrays, or all null with a material map
+  const uint16_t* mat;
+  const Material* tab;
+  Sources S;
+  Monitors M;
+  CpmlDev P;
+  long long t0;
+  float dx;
+};
+// Step t0 + t_offset of every grid: one E launch and one H launch over all grids (blockIdx.z =
+// grid * max_nz + k; cells outside a smaller grid return at once).
+cudaError_t launch_cpml_batch_step(const CpmlSim* sims, int nsims, int max_nx, int max_ny,
+                                   int max_nz, long long t_offset, cudaStream_t st);
+// Deferred DFT of a CPML batch: like launch_dft_fold_batch over CpmlSim arguments.
+cudaError_t launch_dft_fold_cpml_batch(const CpmlSim* sims, int nsims, long long max_np,
+                                       int max_nf, long long t_offset, int n, cudaStream_t st);
+
 // ---------------------------------------------------------------- storage conversion
 // Pitched field array of `storage` (0 FP32, 1 FP16, 2 BF16, 3 FP64) <-> pitched FP32 / FP64.
 cudaError_t convert_field_to_f32(const Grid& g, const void* src, int storage, float scale,

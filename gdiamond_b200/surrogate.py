@@ -94,6 +94,10 @@ class SpectrumSolver:
     """Transmission spectra of designs by batched FDTD (FP32 fields, FP64 DFT sums).
 
     observable: "flux" (default) or "amplitude", as described in the module docstring.
+    boundary: "pml" (default), the reference's graded pseudo-PML of t_pml cells in the
+    coefficients in front of never-updated faces; or "cpml", CPML layers of t_pml cells on every
+    face (fdtd_set_cpml) with vacuum coefficients, which reflect far less, and the flux plane
+    moved in front of the top layer (z = Nz - t_pml - 2 unless monitor_k is given).
 
     Simulations are created once (`group` of them) and reused: each group of designs gets new
     permittivities, a reset, and one persistent batched run of T steps replayed from a CUDA
@@ -102,12 +106,17 @@ class SpectrumSolver:
     """
 
     def __init__(self, shape=SHAPE, T=T_STEPS, n_freqs=N_FREQS, group=256, storage="f32",
-                 source_k=SOURCE_K, monitor_k=MONITOR_K, t_pml=10, observable="flux", device=0):
+                 source_k=SOURCE_K, monitor_k=None, t_pml=10, observable="flux", device=0,
+                 boundary="pml"):
         import torch
         if observable not in ("flux", "amplitude"):
             raise ValueError("observable is 'flux' or 'amplitude'")
+        if boundary not in ("pml", "cpml"):
+            raise ValueError("boundary is 'pml' (the reference's graded pseudo-PML) or 'cpml'")
         self.shape, self.T, self.group, self.storage = tuple(shape), int(T), int(group), storage
-        self.t_pml, self.observable = int(t_pml), observable
+        self.t_pml, self.observable, self.boundary = int(t_pml), observable, boundary
+        if monitor_k is None:  # CPML: the flux plane two cells in front of the top layer
+            monitor_k = MONITOR_K if boundary == "pml" else self.shape[2] - self.t_pml - 2
         self.source_k, self.monitor_k, self.device = int(source_k), int(monitor_k), device
         self.freqs = W.source_band(n_freqs)
         self.wave = W.gaussian_wave(self.T)
@@ -123,6 +132,8 @@ class SpectrumSolver:
 
     def _make(self):
         sim = Simulation(*self.shape, storage=self.storage, device=self.device)
+        if self.boundary == "cpml":
+            sim.set_cpml(thickness=self.t_pml)
         sim.set_sources([dict(component="Jx", kind=SRC_PLANE_Z, k=self.source_k, wave=self.wave)])
         fid = sim.add_flux_monitor(self.monitor_k, self.freqs)
         self._ids[id(sim)] = (fid, sim.flux_monitor_ids(fid)[0])
@@ -146,11 +157,15 @@ class SpectrumSolver:
         ex[:] = e[:, 0] + 1j * e[:, 1]
         return ex, flux
 
+    def _pml_cells(self):
+        """Thickness of the graded pseudo-PML in the coefficients (none under CPML layers)."""
+        return self.t_pml if self.boundary == "pml" else 0
+
     def empty(self):
         """(Ex plane sum, flux) of the grid without a box (the normalisation)."""
         if self._empty is None:
             sim = self._make()
-            sim.set_permittivity(None, t_pml=self.t_pml)
+            sim.set_permittivity(None, t_pml=self._pml_cells())
             sim.step(self.T)
             sim.sync()
             ex, flux = self._measure([sim])
@@ -173,7 +188,7 @@ class SpectrumSolver:
                 self.sims.append(self._make())
             sims = self.sims[:nb]
             for sim, p in zip(sims, padded):
-                sim.set_permittivity(design_eps(p, self.shape), t_pml=self.t_pml)
+                sim.set_permittivity(design_eps(p, self.shape), t_pml=self._pml_cells())
                 sim.reset()
             for sim in sims:
                 sim.sync()

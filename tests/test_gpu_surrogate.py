@@ -54,6 +54,36 @@ def test_solver_matches_oracle_and_unit_transmission():
     sol.close()
 
 
+def test_cpml_solver_matches_single_grids_and_unit_transmission():
+    """boundary="cpml": CPML layers on every face, vacuum coefficients, flux plane in front of
+    the top layer.  The batched CPML solver's fluxes equal a single grid's (per-step monitor
+    accumulation) to the reduction's rounding, and a box of eps 1 transmits exactly 1."""
+    from gdiamond_b200 import SRC_PLANE_Z, Simulation
+    sol = S.SpectrumSolver(shape=SHAPE, T=T, n_freqs=NF, group=3, source_k=SRC_K, t_pml=PML,
+                           boundary="cpml")
+    assert sol.monitor_k == SHAPE[2] - PML - 2
+    designs = S.sample_designs(3, seed=6, shape=SHAPE)
+    designs[2, 5] = 1.0
+    ex, flux = sol.measure(designs)
+    for p, got in zip(designs[:2], flux[:2]):
+        sim = Simulation(*SHAPE)
+        sim.set_cpml(thickness=PML)
+        sim.set_permittivity(S.design_eps(p, SHAPE), t_pml=0)
+        sim.set_sources([dict(component="Jx", kind=SRC_PLANE_Z, k=SRC_K, wave=sol.wave)])
+        fid = sim.add_flux_monitor(sol.monitor_k, sol.freqs)
+        sim.step(T)
+        sim.sync()
+        assert sim.config()["kernel"] == "cpml"
+        want = sim.get_flux(fid)
+        sim.close()
+        assert np.abs(want).max() > 0
+        assert np.array_equal(got, want)
+    spec = sol.to_spectra(ex, flux)
+    assert np.allclose(spec[2], 1.0, rtol=0, atol=1e-12)
+    assert np.all(np.abs(spec[:2] - 1).max(axis=1) > 1e-3)
+    sol.close()
+
+
 def test_surrogate_gain_over_solver():
     sol = solver()
     train = S.sample_designs(768, seed=1, shape=SHAPE)
