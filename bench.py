@@ -345,7 +345,8 @@ def run_ours(args):
     sim.set_coefficients(coefs)
     sim.set_fast_path(not args.no_fast_path)
     if args.cpml:
-        sim.set_cpml(thickness=args.cpml)  # per-step E/H kernels with CPML layers
+        # the tiled kernel plus the shell companion (per-step kernels when the grid is small)
+        sim.set_cpml(thickness=args.cpml)
     sim.set_sources(src)
     mid = sim.add_dft_monitor("Ez", nz // 2, freqs, scale=1.0)
     stream = torch.cuda.Stream()
@@ -423,7 +424,7 @@ def run_ours(args):
     hbm, kind = peaks()
     cells_per_launch = ncell * cfg["blt"]
     achieved = B_ALG * cells_per_launch / (launch_ms / 1e3) / 1e9
-    traffic = traffic_from_profile(cfg) if shape == SHAPE else None
+    traffic = traffic_from_profile(cfg) if shape == SHAPE and not args.cpml else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -465,9 +466,10 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded shapes of the workload; no dataset)",
-        "config": {"workload": WORKLOAD if (shape, T_run) == (SHAPE, T_STEPS) else
-                   f"fdtd3d_{nx}x{ny}x{nz}_vacuum_gaussJz_T{T_run}_dft8_zplane",
-                   "grid": list(shape), "timesteps": T_run,
+        "config": {"workload": (WORKLOAD if (shape, T_run) == (SHAPE, T_STEPS) else
+                                f"fdtd3d_{nx}x{ny}x{nz}_vacuum_gaussJz_T{T_run}_dft8_zplane")
+                   + (f"_cpml{args.cpml}" if args.cpml else ""),
+                   "grid": list(shape), "timesteps": T_run, "cpml_layers": args.cpml,
                    "dft_freqs": N_FREQS, "kernel": cfg["kernel"], "width": cfg.get("width"),
                    "blt": cfg["blt"],
                    "tile_rows": cfg["tile_rows"], "z_chunks": cfg["z_chunks"],

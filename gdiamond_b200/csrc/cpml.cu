@@ -83,13 +83,14 @@ __device__ __forceinline__ bool interior(const Grid& g, int i, int j, int k) {
   return i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2;
 }
 
-// E update of interior cell (i, j, k) at step t, in place.
-__device__ __forceinline__ void e_cell(const Grid& g, const FieldPtrs& F, const float* const* A,
-                                       const uint16_t* mat, const Material* tab,
-                                       const Sources& S, long long t, float dx, const CpmlDev& P,
-                                       int i, int j, int k) {
+// E update of interior cell (i, j, k) at step t: E and H of step t from Fi, the new E into Fo
+// (Fi == Fo: in place).
+__device__ __forceinline__ void e_cell(const Grid& g, const FieldPtrs& Fi, const FieldPtrs& Fo,
+                                       const float* const* A, const uint16_t* mat,
+                                       const Material* tab, const Sources& S, long long t,
+                                       float dx, const CpmlDev& P, int i, int j, int k) {
   const long long sy = g.pitch, sz = g.plane, idx = i + j * sy + k * sz;
-  float* const* f = F.f;
+  float* const* f = Fi.f;
   const float hx = f[3][idx], hy = f[4][idx], hz = f[5][idx];
   const float dyHz = sub(hz, f[5][idx - sy]), dzHy = sub(hy, f[4][idx - sz]);
   const float dzHx = sub(hx, f[3][idx - sz]), dxHz = sub(hz, f[5][idx - 1]);
@@ -120,18 +121,20 @@ __device__ __forceinline__ void e_cell(const Grid& g, const FieldPtrs& F, const 
   }
   float ca[3], cb[3];
   e_coefs(A, mat, tab, idx, ca, cb);
-  f[0][idx] = yee(ca[0], f[0][idx], cb[0], cx);
-  f[1][idx] = yee(ca[1], f[1][idx], cb[1], cy);
-  f[2][idx] = yee(ca[2], f[2][idx], cb[2], cz);
+  const float ex = f[0][idx], ey = f[1][idx], ez = f[2][idx];
+  Fo.f[0][idx] = yee(ca[0], ex, cb[0], cx);
+  Fo.f[1][idx] = yee(ca[1], ey, cb[1], cy);
+  Fo.f[2][idx] = yee(ca[2], ez, cb[2], cz);
 }
 
-// H update of interior cell (i, j, k) at step t, in place (after every E update of the step).
-__device__ __forceinline__ void h_cell(const Grid& g, const FieldPtrs& F, const float* const* A,
-                                       const uint16_t* mat, const Material* tab,
-                                       const Sources& S, long long t, float dx, const CpmlDev& P,
-                                       int i, int j, int k) {
+// H update of interior cell (i, j, k) at step t, after every E update of the step: H of step t
+// from Fi, the new E from Fo, the new H into Fo (Fi == Fo: in place).
+__device__ __forceinline__ void h_cell(const Grid& g, const FieldPtrs& Fi, const FieldPtrs& Fo,
+                                       const float* const* A, const uint16_t* mat,
+                                       const Material* tab, const Sources& S, long long t,
+                                       float dx, const CpmlDev& P, int i, int j, int k) {
   const long long sy = g.pitch, sz = g.plane, idx = i + j * sy + k * sz;
-  float* const* f = F.f;
+  float* const* f = Fo.f;
   const float ex = f[0][idx], ey = f[1][idx], ez = f[2][idx];
   const float dzEy = sub(f[1][idx + sz], ey), dyEz = sub(f[2][idx + sy], ez);
   const float dxEz = sub(f[2][idx + 1], ez), dzEx = sub(f[0][idx + sz], ex);
@@ -162,9 +165,10 @@ __device__ __forceinline__ void h_cell(const Grid& g, const FieldPtrs& F, const 
   }
   float da[3], db[3];
   h_coefs(A, mat, tab, idx, da, db);
-  f[3][idx] = yee(da[0], f[3][idx], db[0], cx);
-  f[4][idx] = yee(da[1], f[4][idx], db[1], cy);
-  f[5][idx] = yee(da[2], f[5][idx], db[2], cz);
+  const float hx = Fi.f[3][idx], hy = Fi.f[4][idx], hz = Fi.f[5][idx];
+  Fo.f[3][idx] = yee(da[0], hx, db[0], cx);
+  Fo.f[4][idx] = yee(da[1], hy, db[1], cy);
+  Fo.f[5][idx] = yee(da[2], hz, db[2], cz);
 }
 
 // One grid: grid (ceil(nx/32), ceil(ny/4), nz), block (32, 4); interior cells only.
@@ -172,14 +176,14 @@ __global__ void __launch_bounds__(128) cpml_e(Grid g, FieldPtrs F, CoefRefs A, c
                                               const Material* tab, Sources S, long long t,
                                               float dx, CpmlDev P) {
   const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, k = blockIdx.z;
-  if (interior(g, i, j, k)) e_cell(g, F, A.c, mat, tab, S, t, dx, P, i, j, k);
+  if (interior(g, i, j, k)) e_cell(g, F, F, A.c, mat, tab, S, t, dx, P, i, j, k);
 }
 
 __global__ void __launch_bounds__(128) cpml_h(Grid g, FieldPtrs F, CoefRefs A, const uint16_t* mat,
                                               const Material* tab, Sources S, long long t,
                                               float dx, CpmlDev P) {
   const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, k = blockIdx.z;
-  if (interior(g, i, j, k)) h_cell(g, F, A.c, mat, tab, S, t, dx, P, i, j, k);
+  if (interior(g, i, j, k)) h_cell(g, F, F, A.c, mat, tab, S, t, dx, P, i, j, k);
 }
 
 // Monitor values of cell (i, j) of plane k at step t into the staging rings: the E monitors
@@ -203,7 +207,7 @@ __global__ void __launch_bounds__(128) cpml_e_batch(const CpmlSim* sims, int max
   const int k = (int)(blockIdx.z % max_nz);
   if (i >= s.g.nx || j >= s.g.ny || k >= s.g.nz) return;
   const long long t = s.t0 + t_offset;
-  if (interior(s.g, i, j, k)) e_cell(s.g, s.F, s.coef, s.mat, s.tab, s.S, t, s.dx, s.P, i, j, k);
+  if (interior(s.g, i, j, k)) e_cell(s.g, s.F, s.F, s.coef, s.mat, s.tab, s.S, t, s.dx, s.P, i, j, k);
   if (s.M.n) stage_cell(s, t, i, j, k, true);
 }
 
@@ -214,11 +218,55 @@ __global__ void __launch_bounds__(128) cpml_h_batch(const CpmlSim* sims, int max
   const int k = (int)(blockIdx.z % max_nz);
   if (i >= s.g.nx || j >= s.g.ny || k >= s.g.nz) return;
   const long long t = s.t0 + t_offset;
-  if (interior(s.g, i, j, k)) h_cell(s.g, s.F, s.coef, s.mat, s.tab, s.S, t, s.dx, s.P, i, j, k);
+  if (interior(s.g, i, j, k)) h_cell(s.g, s.F, s.F, s.coef, s.mat, s.tab, s.S, t, s.dx, s.P, i, j, k);
   if (s.M.n) stage_cell(s, t, i, j, k, false);
 }
 
+// The shell companion: blockIdx.x indexes the block list; cells inside `inner` return.
+template <bool H>
+__global__ void __launch_bounds__(128) cpml_region(Grid g, FieldPtrs Fi, FieldPtrs Fo,
+                                                   const uint16_t* mat, const Material* tab,
+                                                   Sources S, Monitors M, CpmlDev P, long long t,
+                                                   float dx, const int4* blocks, CpmlBox inner) {
+  const int4 b = blocks[blockIdx.x];
+  const int i = b.x * 32 + threadIdx.x, j = b.y * 4 + threadIdx.y, k = b.z;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  if (i >= inner.lo[0] && i < inner.hi[0] && j >= inner.lo[1] && j < inner.hi[1] &&
+      k >= inner.lo[2] && k < inner.hi[2])
+    return;
+  const long long idx = i + (long long)j * g.pitch + (long long)k * g.plane;
+  const int c0 = H ? 3 : 0;
+  if (interior(g, i, j, k)) {
+    if (H)
+      h_cell(g, Fi, Fo, nullptr, mat, tab, S, t, dx, P, i, j, k);
+    else
+      e_cell(g, Fi, Fo, nullptr, mat, tab, S, t, dx, P, i, j, k);
+  } else if (Fi.f[c0] != Fo.f[c0]) {  // faces never change: carry them into the output set
+    for (int c = c0; c < c0 + 3; ++c) Fo.f[c][idx] = Fi.f[c][idx];
+  }
+  for (int n = 0; n < M.n; ++n) {
+    const MonitorDev& m = M.m[n];
+    if ((m.comp >= 3) == H && m.k == k) dft_record(m, t, i, j, g, Fo.f[m.comp][idx]);
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_cpml_region(bool h_half, const Grid& g, const FieldPtrs& Fi,
+                               const FieldPtrs& Fo, const uint16_t* mat, const Material* tab,
+                               const Sources& S, const Monitors& M, const CpmlDev& P,
+                               long long t, float dx, const int4* blocks, int nblocks,
+                               const CpmlBox& inner, cudaStream_t st) {
+  if (nblocks <= 0) return cudaSuccess;
+  if (!mat) return cudaErrorInvalidValue;
+  if (h_half)
+    cpml_region<true><<<nblocks, dim3(32, 4), 0, st>>>(g, Fi, Fo, mat, tab, S, M, P, t, dx,
+                                                        blocks, inner);
+  else
+    cpml_region<false><<<nblocks, dim3(32, 4), 0, st>>>(g, Fi, Fo, mat, tab, S, M, P, t, dx,
+                                                         blocks, inner);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_cpml_batch_step(const CpmlSim* sims, int nsims, int max_nx, int max_ny,
                                    int max_nz, long long t_offset, cudaStream_t st) {

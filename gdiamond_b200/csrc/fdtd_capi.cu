@@ -125,6 +125,14 @@ struct fdtd_handle {
   std::vector<int> cpml_slot[3][2];      // host copies of the slot tables (E, H positions)
   std::vector<float> cpml_prof[3][2][3]; // host copies of b, a, 1/kappa
   fdtd::CpmlDev cpml_dev{};
+  // Shell companion of the tiled kernel (cpml_companion): cpml_inner = per axis the [lo, hi)
+  // range of positions whose E and H updates involve no layer, cpml_lo / cpml_hi = the axis has
+  // a layer on that side; a third FP32 field set for the companion's intermediate steps; block
+  // lists of the regions it updates, per depth r.
+  int cpml_inner[3][2] = {};
+  bool cpml_lo[3] = {}, cpml_hi[3] = {};
+  float* cpml_scratch[6] = {};
+  std::map<int, std::pair<int4*, int>> cpml_blocks;
   uint8_t* ublk = nullptr;  // uniform-block map of the lean material (fdtd::build_uniform_blocks)
   int ub[3] = {0, 0, 0};
   std::vector<uint8_t> ublk_host;  // its host copy (tile launch order)
@@ -471,6 +479,16 @@ fdtd_status check_device_error(fdtd_handle* h) {
   return FDTD_OK;
 }
 
+// Releases the shell companion's field set and block lists (rebuilt on demand).
+void cpml_release_companion(fdtd_handle* h) {
+  for (int c = 0; c < 6; ++c) {
+    cudaFree(h->cpml_scratch[c]);
+    h->cpml_scratch[c] = nullptr;
+  }
+  for (auto& kv : h->cpml_blocks) cudaFree(kv.second.first);
+  h->cpml_blocks.clear();
+}
+
 void free_all(fdtd_handle* h) {
   for (int s = 0; s < 2; ++s)
     for (int c = 0; c < 6; ++c) cudaFree(h->F[s][c]);
@@ -484,6 +502,7 @@ void free_all(fdtd_handle* h) {
   cudaFree(h->d_order);
   cudaFree(h->cpml_tab);
   for (int q = 0; q < 12; ++q) cudaFree(h->cpml_psi[q]);
+  cpml_release_companion(h);
   cudaFree(h->f32_stage);
   cudaFree(h->f64_stage);
   for (int m = 0; m < h->nmon; ++m) {
@@ -746,6 +765,102 @@ void drop_monitors(fdtd_handle* h, int first) {
     h->mon[m] = MonitorHost();
   }
   h->nmon = first;
+}
+
+// ------------------------------------------------------------ CPML shell companion
+// With CPML layers the tiled kernel advances the whole grid by k steps with the plain update;
+// its results are right wherever the layers cannot reach within k steps.  One step moves
+// information by at most one cell along each axis (E reads H at i and i-1, H reads E at i and
+// i+1), so after k steps the tiled kernel is wrong only within k cells of the shell (the cells
+// whose own update involves a layer).  The companion recomputes those cells: from the fields
+// of the launch's start (set A) it runs the k steps with the CPML update over regions that
+// shrink towards the shell, the intermediate steps in a third field set, the last into the
+// tiled kernel's output (set B).  W_r = the cells within r of the shell = outside the inner
+// box shrunk by r on every side with a layer.  Step j updates E on W_{e_j}, H on W_{e_j - 1},
+// e_j = 3k - 2(j - 1): each half step needs the previous one on a region one cell deeper, and
+// the last step covers W_{k+2} (E) and W_{k+1} (H), beyond what the tiled kernel got wrong.
+// psi is updated by the companion alone, once per cell and step; monitor values of the
+// recomputed cells are staged again over the tiled kernel's.
+
+// The inner box shrunk by r cells on every side that has a layer.
+fdtd::CpmlBox cpml_inner_box(const fdtd_handle* h, int r) {
+  const int n[3] = {h->g.nx, h->g.ny, h->g.nz};
+  fdtd::CpmlBox b;
+  for (int a = 0; a < 3; ++a) {
+    b.lo[a] = h->cpml_lo[a] ? h->cpml_inner[a][0] + r : 0;
+    b.hi[a] = h->cpml_hi[a] ? h->cpml_inner[a][1] - r : n[a];
+    if (b.hi[a] < b.lo[a]) b.hi[a] = b.lo[a];
+  }
+  return b;
+}
+
+// The companion pays off when the inner box of its deepest region still holds most cells.
+bool cpml_companion_fits(const fdtd_handle* h, int k) {
+  const fdtd::CpmlBox b = cpml_inner_box(h, 3 * k);
+  double inner = 1.0;
+  for (int a = 0; a < 3; ++a) inner *= (double)(b.hi[a] - b.lo[a]);
+  return inner >= 0.4 * (double)h->g.nx * h->g.ny * h->g.nz;
+}
+
+// Device list of the 32 x 4-cell blocks (x tile, y tile, plane) that hold cells of W_r.
+fdtd_status cpml_region_blocks(fdtd_handle* h, int r, std::pair<int4*, int>* out) {
+  auto it = h->cpml_blocks.find(r);
+  if (it != h->cpml_blocks.end()) {
+    *out = it->second;
+    return FDTD_OK;
+  }
+  const fdtd::CpmlBox b = cpml_inner_box(h, r);
+  const int ntx = (h->g.nx + 31) / 32, nty = (h->g.ny + 3) / 4;
+  std::vector<int4> v;
+  for (int k = 0; k < h->g.nz; ++k) {
+    const bool zin = k >= b.lo[2] && k < b.hi[2];
+    for (int ty = 0; ty < nty; ++ty)
+      for (int tx = 0; tx < ntx; ++tx) {
+        const bool inside = zin && 32 * tx >= b.lo[0] && 32 * tx + 32 <= b.hi[0] &&
+                            4 * ty >= b.lo[1] && 4 * ty + 4 <= b.hi[1];
+        if (!inside) v.push_back(make_int4(tx, ty, k, 0));
+      }
+  }
+  int4* d = nullptr;
+  CUDA_TRY(h, cudaMalloc(&d, std::max<size_t>(v.size(), 1) * sizeof(int4)));
+  CUDA_TRY(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  h->cpml_blocks[r] = {d, (int)v.size()};
+  *out = h->cpml_blocks[r];
+  return FDTD_OK;
+}
+
+// The companion of one tiled launch of k steps from field set `src` (step t) to `dst`.
+fdtd_status cpml_companion(fdtd_handle* h, int k, int src, int dst, long long t,
+                           const fdtd::Sources& S, const fdtd::Monitors& M, cudaStream_t st,
+                           int* launches) {
+  if (k > 1 && !h->cpml_scratch[0]) {
+    for (int c = 0; c < 6; ++c)
+      CUDA_TRY(h, cudaMalloc(&h->cpml_scratch[c], h->cells * sizeof(float)));
+  }
+  fdtd::FieldPtrs A, B, C;
+  for (int c = 0; c < 6; ++c) {
+    A.f[c] = h->F[src][c];
+    B.f[c] = h->F[dst][c];
+    C.f[c] = h->cpml_scratch[c];
+  }
+  for (int j = 1; j <= k; ++j) {
+    const fdtd::FieldPtrs& Fi = j == 1 ? A : C;
+    const fdtd::FieldPtrs& Fo = j == k ? B : C;
+    const int re = 3 * k - 2 * (j - 1), rh = re - 1;
+    std::pair<int4*, int> le, lh;
+    fdtd_status s = cpml_region_blocks(h, re, &le);
+    if (s == FDTD_OK) s = cpml_region_blocks(h, rh, &lh);
+    if (s != FDTD_OK) return s;
+    const long long tj = t + j - 1;
+    CUDA_TRY(h, fdtd::launch_cpml_region(false, h->g, Fi, Fo, h->mat, h->table, S, M,
+                                         h->cpml_dev, tj, h->desc.dx, le.first, le.second,
+                                         cpml_inner_box(h, re), st));
+    CUDA_TRY(h, fdtd::launch_cpml_region(true, h->g, Fi, Fo, h->mat, h->table, S, M,
+                                         h->cpml_dev, tj, h->desc.dx, lh.first, lh.second,
+                                         cpml_inner_box(h, rh), st));
+    *launches += 2;
+  }
+  return FDTD_OK;
 }
 
 }  // namespace
@@ -1072,9 +1187,20 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
   }
   fdtd_status s = ensure_tables(h, h->t + T);
   if (s != FDTD_OK) return s;
-  if (h->cpml_on) {  // CPML layers: one E and one H kernel per step, monitors per step
+  // CPML layers: the tiled kernel with the shell companion when the grid is large enough for
+  // it (and the caller did not ask for the naive kernel), else one E and one H kernel per step
+  // over the whole grid, monitors per step.
+  bool companion = false;
+  if (h->cpml_on) {
     if (h->storage != FDTD_STORE_F32)
       return fail(h, FDTD_ERR_UNSUPPORTED, "CPML layers need FP32 field storage");
+    if (h->desc.kernel != FDTD_KERNEL_NAIVE && h->coef_mode == kCoefMaterial &&
+        cpml_companion_fits(h, 1)) {
+      if (!h->cfg_ready && (s = autotune(h, st)) != FDTD_OK) return s;
+      companion = cpml_companion_fits(h, h->cfg.blt);
+    }
+  }
+  if (h->cpml_on && !companion) {
     fdtd::FieldPtrs F;
     for (int c = 0; c < 6; ++c) F.f[c] = h->F[h->cur][c];
     const bool matm = h->coef_mode == kCoefMaterial;
@@ -1155,6 +1281,10 @@ fdtd_status fdtd_step(fdtd_handle* h, int64_t T, void* stream) {
       h->fault_tile[0] = h->fault_tile[1] = h->fault_tile[2] = -1;  // the hook fires once
       CUDA_TRY(h, launch_any(cc, a, h->g, st));
       ++launches;
+      if (companion &&
+          (s = cpml_companion(h, cc.blt, h->cur, h->cur ^ 1, h->t, S, M, st, &launches)) !=
+              FDTD_OK)
+        return s;
       h->cur ^= 1;
       h->t += cc.blt;
       left -= cc.blt;
@@ -1391,6 +1521,7 @@ fdtd_status fdtd_set_cpml(fdtd_handle* h, const fdtd_cpml_desc* d) {
     cudaFree(h->cpml_psi[q]);
     h->cpml_psi[q] = nullptr;
   }
+  cpml_release_companion(h);
   h->cpml_on = false;
   if (!d) return FDTD_OK;
   if (d->thickness < 1 || !(d->order >= 0) || !(d->reflection > 0 && d->reflection < 1) ||
@@ -1446,6 +1577,20 @@ fdtd_status fdtd_set_cpml(fdtd_handle* h, const fdtd_cpml_desc* d) {
     }
     CUDA_TRY(h, cudaMemset(h->cpml_psi[q], 0, pb));
     (q < 6 ? h->cpml_dev.psi_e[q] : h->cpml_dev.psi_h[q - 6]) = h->cpml_psi[q];
+  }
+  // positions whose updates involve no layer, per axis (the shell companion's inner box)
+  for (int a = 0; a < 3; ++a) {
+    int lo = 0, hi = n[a];
+    for (int p = 0; p < n[a]; ++p) {
+      const bool in = h->cpml_slot[a][0][p] >= 0 || h->cpml_slot[a][1][p] >= 0;
+      if (!in) continue;
+      if (2 * p < n[a]) lo = std::max(lo, p + 1);
+      else hi = std::min(hi, p);
+    }
+    h->cpml_inner[a][0] = lo;
+    h->cpml_inner[a][1] = hi;
+    h->cpml_lo[a] = lo > 0;
+    h->cpml_hi[a] = hi < n[a];
   }
   h->cpml_on = true;
   return FDTD_OK;

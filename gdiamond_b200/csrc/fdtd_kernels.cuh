@@ -65,6 +65,19 @@ struct CpmlSim {
 // grid * max_nz + k; cells outside a smaller grid return at once).
 cudaError_t launch_cpml_batch_step(const CpmlSim* sims, int nsims, int max_nx, int max_ny,
                                    int max_nz, long long t_offset, cudaStream_t st);
+// The shell companion of the tiled kernel under CPML layers (cpml.cu): one half step (E, or
+// H with h_half) of step t over the cells of `blocks` (int4 {x tile of 32 cells, y tile of 4
+// rows, plane k, unused}) that lie outside the box `inner` ([lo, hi) per axis x, y, z).  Reads
+// the fields of step t from Fi (and, for H, the new E from Fo), writes Fo; face cells are
+// copied; the half step's monitor values are staged.  Material maps only.
+struct CpmlBox {
+  int lo[3], hi[3];
+};
+cudaError_t launch_cpml_region(bool h_half, const Grid& g, const FieldPtrs& Fi,
+                               const FieldPtrs& Fo, const uint16_t* mat, const Material* tab,
+                               const Sources& S, const Monitors& M, const CpmlDev& P,
+                               long long t, float dx, const int4* blocks, int nblocks,
+                               const CpmlBox& inner, cudaStream_t st);
 // Deferred DFT of a CPML batch: like launch_dft_fold_batch over CpmlSim arguments.
 cudaError_t launch_dft_fold_cpml_batch(const CpmlSim* sims, int nsims, long long max_np,
                                        int max_nf, long long t_offset, int n, cudaStream_t st);

@@ -179,9 +179,14 @@ fdtd_status fdtd_flux_monitor_ids(const fdtd_handle* h, int32_t flux_id, int32_t
  * rho^order, alpha = alpha_max (1 - rho); E differences use rho at integer positions, H
  * differences at half-integer ones.  Outside the layers the update is the reference's, bit for
  * bit.  Give the interior material's coefficients (e.g. fdtd_set_permittivity with t_pml = 0):
- * the CPML replaces the grading.  With layers on, fdtd_step runs one E and one H kernel per step
- * (FP32 storage only); the psi fields live only in the slabs of their axis.  NULL turns the
- * layers off. */
+ * the CPML replaces the grading.  FP32 storage only; the psi fields live only in the slabs of
+ * their axis.  With layers on, fdtd_step runs the tiled kernel over the whole grid and a shell
+ * companion that recomputes, per tiled launch of k steps, the cells the layers can reach within
+ * those steps (when the cells more than 3k from the layers are at least 40 % of the grid and the
+ * handle's kernel is not FDTD_KERNEL_NAIVE); otherwise one E and one H kernel per step over the
+ * grid.  Both give the same fields and monitor sums bit for bit.  fdtd_batch_step advances a
+ * batch whose simulations all have layers with one E and one H launch per step over every
+ * grid.  NULL turns the layers off. */
 typedef struct fdtd_cpml_desc {
   int32_t thickness;   /* cells per face (L); each axis with layers needs >= 2 L + 2 cells */
   int32_t faces;       /* bit mask of faces with a layer: 1 -x, 2 +x, 4 -y, 8 +y, 16 -z, 32 +z */

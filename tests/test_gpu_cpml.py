@@ -22,8 +22,8 @@ pytestmark = pytest.mark.gpu
 DX, DT = float(np.float32(0.1)), float(np.float32(0.05))
 
 
-def make(shape, coefs, src, L, faces=63, kappa_max=1.5):
-    sim = gd.Simulation(*shape)
+def make(shape, coefs, src, L, faces=63, kappa_max=1.5, kernel="auto", blt=0):
+    sim = gd.Simulation(*shape, kernel=kernel, blt=blt)
     sim.set_coefficients(coefs)
     sim.set_cpml(thickness=L, faces=faces, kappa_max=kappa_max)
     if src:
@@ -46,8 +46,12 @@ def test_profile_tables_match_formula():
     sim.close()
 
 
-@pytest.mark.parametrize("faces,percell", [(63, False), (16 | 32, False), (63, True)])
-def test_cpml_fields_match_oracle(faces, percell):
+@pytest.mark.parametrize("faces,percell,kernel", [(63, False, "auto"), (16 | 32, False, "auto"),
+                                                  (16 | 32, False, "naive"), (63, True, "auto")])
+def test_cpml_fields_match_oracle(faces, percell, kernel):
+    """Layers on every face (too little interior for the shell companion: per-step kernels),
+    on the z faces only (the tiled kernel with the shell companion, or per-step kernels when the
+    naive kernel is asked for), and with per-cell coefficients (per-step kernels)."""
     shape, T, L = ((48, 40, 44) if percell else (40, 36, 44)), 60, 6
     nx, ny, nz = shape
     eps = W.spheres_eps(shape, n_spheres=3, r_range=(3, 5), eps_range=(2.0, 4.0), seed=9)
@@ -59,11 +63,13 @@ def test_cpml_fields_match_oracle(faces, percell):
     w = W.gaussian_wave(T, delay=15.0, width=5.0, period=8.0)
     src = [dict(component="Jz", wave=w, i=nx // 2, j=ny // 2, k=nz // 2),
            dict(component="Jx", wave=w * np.float32(0.2), k=nz - 9, kind=gd.SRC_PLANE_Z)]
-    sim = make(shape, coefs, src, L, faces=faces)
+    companion = faces == 16 | 32 and kernel == "auto"
+    # BLT 2: the interior left beyond 3 BLT cells from the z layers is still most of this grid
+    sim = make(shape, coefs, src, L, faces=faces, kernel=kernel, blt=2 if companion else 0)
     assert (sim.material_count() == 0) == percell
     sim.step(T)
     sim.sync()
-    assert sim.config()["kernel"] == "cpml"
+    assert sim.config()["kernel"] == ("tiled" if companion else "cpml")
     F = sim.fields()
     F_ref = cpml.run(shape, coefs, T, sim.cpml_tables(), sources=[osrc(s) for s in src], dx=DX)
     assert_fields_match(F, F_ref, f"cpml faces={faces} percell={percell}")
@@ -215,3 +221,49 @@ def test_cpml_batch_rejects_mixed_boundaries():
         gd.Batch([a, c])
     a.close()
     c.close()
+
+
+def _companion_pair(shape, L, blt, kernel):
+    """A CPML grid with sources inside a layer, near the shell and in the interior, a flux
+    monitor and an Ez DFT monitor on a plane that crosses the side layers."""
+    nx, ny, nz = shape
+    eps = W.spheres_eps(shape, n_spheres=4, r_range=(4, 8), eps_range=(2.0, 6.0), seed=4)
+    sim = gd.Simulation(*shape, kernel=kernel, blt=blt if kernel != "naive" else 0)
+    sim.set_coefficients(W.reference_coefficients(shape, eps_re=eps, t_pml=0))
+    sim.set_cpml(thickness=L, kappa_max=1.5)
+    T = 200
+    w = W.gaussian_wave(T, delay=12.0, width=4.0, period=6.0)
+    sim.set_sources([dict(component="Jx", wave=w, k=L + 3, kind=gd.SRC_PLANE_Z),
+                     dict(component="Jz", wave=w * np.float32(0.5), i=nx // 2, j=ny // 3,
+                          k=nz // 2),
+                     dict(component="Jy", wave=w * np.float32(0.7), i=2, j=ny // 2, k=nz // 3),
+                     dict(component="My", wave=w * np.float32(0.2), i=nx - 5, j=ny // 2,
+                          k=nz // 2)])
+    freqs = W.source_band(4, period=6.0, width=4.0)
+    mons = [("flux", sim.add_flux_monitor(nz - L - 4, freqs)),
+            ("dft", sim.add_dft_monitor("Ez", nz // 2, freqs)),
+            ("dft", sim.add_dft_monitor("Hx", 3, freqs))]
+    return sim, mons
+
+
+@pytest.mark.parametrize("blt", [1, 2, 3])
+def test_cpml_shell_companion_matches_per_step_path(blt):
+    """With CPML layers on a grid large enough, the tiled kernel advances the whole grid and
+    the shell companion recomputes the cells the layers reach; fields, psi (through continued
+    stepping), DFT sums and fluxes equal the per-step CPML path's bit for bit, over step calls
+    that are not multiples of BLT."""
+    shape, L = (128, 112, 120), 6
+    ref, rm = _companion_pair(shape, L, blt, "naive")
+    sim, sm = _companion_pair(shape, L, blt, "auto")
+    for T in (2 * blt + 1, 23, 40):
+        ref.step(T)
+        sim.step(T)
+        ref.sync()
+        sim.sync()
+        assert ref.config()["kernel"] == "cpml"
+        assert sim.config()["kernel"] == "tiled" and sim.config()["blt"] == blt
+        assert_fields_match(sim.fields(), ref.fields(), f"companion blt={blt} T={T}")
+        for got, want in zip(_read(sim, sm), _read(ref, rm)):
+            assert np.array_equal(got, want)
+    ref.close()
+    sim.close()
