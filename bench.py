@@ -879,7 +879,8 @@ def batched_results(args, storages, one_at_a_time=True):
 def run_surrogate(args):
     """Learned surrogate: 4096 training + 512 held-out designs (a dielectric box in a 96^3
     grid, six numbers each; --train for more), Poynting-flux transmission spectra at 64
-    frequencies from the batched FP32 solver (CUDA graph, T=2000); an ensemble of 4 MLPs
+    frequencies from the batched FP32 solver (CUDA graph, T=2000; CPML layers on every face,
+    or with --boundary pml the reference's graded pseudo-PML); an ensemble of 4 MLPs
     6->256->256->256->64 trained on the GPU (BF16 tensor-core GEMMs, FP32 accumulation, Adam
     lr 1e-3, 200 epochs); held-out spectral error against FDTD with and without the
     ensemble-disagreement fallback, and designs/s of surrogate-with-fallback against the
@@ -1100,8 +1101,9 @@ def main():
                          "disagreement of a first ensemble (active sampling)")
     ap.add_argument("--epochs", type=int, default=200, help="surrogate: training epochs")
     ap.add_argument("--mlp-batch", type=int, default=64, help="surrogate: minibatch rows")
-    ap.add_argument("--boundary", default="pml", choices=["pml", "cpml"],
-                    help="surrogate: the reference's graded pseudo-PML or CPML layers")
+    ap.add_argument("--boundary", default="cpml", choices=["pml", "cpml"],
+                    help="surrogate: CPML layers on every face (default) or the reference's "
+                         "graded pseudo-PML")
     ap.add_argument("--observable", default="flux", choices=["flux", "amplitude"],
                     help="surrogate: transmission observable")
     ap.add_argument("--surrogate-data", default="",
