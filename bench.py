@@ -936,7 +936,8 @@ def run_surrogate(args):
     out["fallback_buckets"] = "batch sizes padded to powers of two from 4 up to the group"
     sur = S.Surrogate(members=4, seed=0)
     t0 = time.perf_counter()
-    losses = sur.fit(train, y_train, epochs=args.epochs, batch=args.mlp_batch, lr=1e-3, seed=0)
+    losses = sur.fit(train, y_train, epochs=args.epochs, batch=args.mlp_batch, lr=args.mlp_lr,
+                     seed=0)
     t_fit = time.perf_counter() - t0
     mean, sd = sur.predict(test)
     err = S.spectral_error(mean, y_test)
@@ -945,7 +946,7 @@ def run_surrogate(args):
     t0 = time.perf_counter()
     sol.warm()  # every bucketed fallback batch size created, tuned and captured once
     t_warm = time.perf_counter() - t0
-    for thr in (0.01, 0.02, 0.05):
+    for thr in (0.01, 0.02, 0.03, 0.05):
         rates = []
         for _ in range(3):  # three timed evaluations: the run-to-run spread of the rate
             spec, mask, t_s, t_f = sur.evaluate(test, sol, threshold=thr)
@@ -958,6 +959,14 @@ def run_surrogate(args):
                            "spectral_err_mean": float(e.mean()),
                            "spectral_err_p95": float(np.quantile(e, 0.95)),
                            "spectral_err_max": float(e.max())}
+    # the fastest threshold whose mean held-out error stays within 2 %
+    ok = [(v["designs_per_s"], k) for k, v in res.items() if v["spectral_err_mean"] <= 0.02]
+    best_2pct = None
+    if ok:
+        r, k = max(ok)
+        best_2pct = {"threshold": float(k), "designs_per_s": r,
+                     "speedup_vs_batched_solver": res[k]["speedup_vs_batched_solver"],
+                     "spectral_err_mean": res[k]["spectral_err_mean"]}
     # inference throughput on device buffers (1M designs), CUDA events on the call's stream
     n_inf = 1 << 20
     x = torch.empty((n_inf, 6), device="cuda").uniform_(-1, 1)
@@ -981,6 +990,7 @@ def run_surrogate(args):
     out["inference_1M"] = {"designs_per_s": n_inf / sec, "tflops": flop / sec / 1e12,
                            "frac_of_bf16_peak": flop / sec / 1e12 / pk["bf16_tflops"]}
     out["surrogate"] = {"observable": args.observable, "boundary": args.boundary,
+                        "adam_lr": args.mlp_lr,
                         "flux_plane": sol.monitor_k, "train_seconds": t_fit,
                         "bucket_warmup_seconds": t_warm,
                         "epochs": args.epochs, "batch": args.mlp_batch,
@@ -991,7 +1001,7 @@ def run_surrogate(args):
                         "baseline_mean_spectrum_err": float(S.spectral_error(
                             np.broadcast_to(y_train.mean(0), y_test.shape), y_test).mean()),
                         "disagreement_median": float(np.median(dis)),
-                        "with_fallback": res}
+                        "with_fallback": res, "fastest_within_2pct_err": best_2pct}
     sur.close()
     sol.close()
     line = {"metric": "designs/s (surrogate with FDTD fallback vs batched solver) at stated "
@@ -1101,6 +1111,8 @@ def main():
                          "disagreement of a first ensemble (active sampling)")
     ap.add_argument("--epochs", type=int, default=200, help="surrogate: training epochs")
     ap.add_argument("--mlp-batch", type=int, default=64, help="surrogate: minibatch rows")
+    ap.add_argument("--mlp-lr", type=float, default=1e-3,
+                    help="surrogate: Adam learning rate of the ensemble (the config's 1e-3)")
     ap.add_argument("--boundary", default="cpml", choices=["pml", "cpml"],
                     help="surrogate: CPML layers on every face (default) or the reference's "
                          "graded pseudo-PML")

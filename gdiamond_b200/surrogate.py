@@ -94,10 +94,10 @@ class SpectrumSolver:
     """Transmission spectra of designs by batched FDTD (FP32 fields, FP64 DFT sums).
 
     observable: "flux" (default) or "amplitude", as described in the module docstring.
-    boundary: "pml" (default), the reference's graded pseudo-PML of t_pml cells in the
-    coefficients in front of never-updated faces; or "cpml", CPML layers of t_pml cells on every
-    face (fdtd_set_cpml) with vacuum coefficients, which reflect far less, and the flux plane
-    moved in front of the top layer (z = Nz - t_pml - 2 unless monitor_k is given).
+    boundary: "pml" (default), the reference's graded pseudo-PML of t_pml cells (10) in the
+    coefficients in front of never-updated faces; or "cpml", CPML layers of t_pml cells (8) on
+    every face (fdtd_set_cpml) with vacuum coefficients, which reflect far less.  With 8-cell
+    layers the source plane z = 10 and the flux plane z = 86 of a 96^3 grid stay outside them.
 
     Simulations are created once (`group` of them) and reused: each group of designs gets new
     permittivities, a reset, and one persistent batched run of T steps replayed from a CUDA
@@ -106,18 +106,22 @@ class SpectrumSolver:
     """
 
     def __init__(self, shape=SHAPE, T=T_STEPS, n_freqs=N_FREQS, group=256, storage="f32",
-                 source_k=SOURCE_K, monitor_k=None, t_pml=10, observable="flux", device=0,
-                 boundary="pml"):
+                 source_k=SOURCE_K, monitor_k=MONITOR_K, t_pml=None, observable="flux",
+                 device=0, boundary="pml"):
         import torch
         if observable not in ("flux", "amplitude"):
             raise ValueError("observable is 'flux' or 'amplitude'")
         if boundary not in ("pml", "cpml"):
             raise ValueError("boundary is 'pml' (the reference's graded pseudo-PML) or 'cpml'")
         self.shape, self.T, self.group, self.storage = tuple(shape), int(T), int(group), storage
+        if t_pml is None:
+            t_pml = 10 if boundary == "pml" else 8
         self.t_pml, self.observable, self.boundary = int(t_pml), observable, boundary
-        if monitor_k is None:  # CPML: the flux plane two cells in front of the top layer
-            monitor_k = MONITOR_K if boundary == "pml" else self.shape[2] - self.t_pml - 2
         self.source_k, self.monitor_k, self.device = int(source_k), int(monitor_k), device
+        nz = self.shape[2]
+        if boundary == "cpml" and not (self.t_pml <= self.source_k and
+                                       self.monitor_k <= nz - 2 - self.t_pml):
+            raise ValueError("the source and flux planes must lie outside the CPML layers")
         self.freqs = W.source_band(n_freqs)
         self.wave = W.gaussian_wave(self.T)
         self.sims = []

@@ -56,12 +56,14 @@ def test_solver_matches_oracle_and_unit_transmission():
 
 def test_cpml_solver_matches_single_grids_and_unit_transmission():
     """boundary="cpml": CPML layers on every face, vacuum coefficients, flux plane in front of
-    the top layer.  The batched CPML solver's fluxes equal a single grid's (per-step monitor
+    the top layer (a plane inside a layer is refused).  The batched CPML solver's fluxes equal a single grid's (per-step monitor
     accumulation) to the reduction's rounding, and a box of eps 1 transmits exactly 1."""
     from gdiamond_b200 import SRC_PLANE_Z, Simulation
     sol = S.SpectrumSolver(shape=SHAPE, T=T, n_freqs=NF, group=3, source_k=SRC_K, t_pml=PML,
-                           boundary="cpml")
-    assert sol.monitor_k == SHAPE[2] - PML - 2
+                           monitor_k=SHAPE[2] - PML - 2, boundary="cpml")
+    with pytest.raises(ValueError):  # a flux plane inside the top layer
+        S.SpectrumSolver(shape=SHAPE, T=T, source_k=SRC_K, t_pml=PML, monitor_k=SHAPE[2] - PML,
+                         boundary="cpml")
     designs = S.sample_designs(3, seed=6, shape=SHAPE)
     designs[2, 5] = 1.0
     ex, flux = sol.measure(designs)
