@@ -703,37 +703,47 @@ void cpml_profile(const fdtd_cpml_desc& d, int n, bool lo, bool hi, double dx, b
 // will run the mixed z-march (a source or a non-uniform block in their staged box; the device
 // test is tile_uniform in k_tiled2.cuh) first, then the lean-only ones.  Null when there is
 // nothing to reorder.
+// Whether tile (bx, by, bz) of h under config c (z-chunks of zlen planes) can run the lean-only
+// z-march: no source in or next to its staged box and every cell of the box in a uniform block
+// of the lean material -- the device's tile_uniform, decided on the host for launch order.
+bool tile_is_lean(const fdtd_handle* h, const fdtd::TiledConfig& c, int bx, int by, int bz,
+                  int zlen) {
+  if (!(c.width == 64 || c.pairs32) || h->ublk_host.empty() || !h->lean_enable) return false;
+  const Grid& g = h->g;
+  const int W = c.pairs32 ? 32 : c.width, B = c.blt;
+  const int SX = fdtd::tiled2_sx_w(W, B), SY = fdtd::tiled_sy(B, c.rows);
+  const int XB = fdtd::tiled2_xbase(B), WB = W + fdtd::kTiled2BoxPad;
+  const int z0 = bz * zlen, X8 = (bx * SX + XB) & ~7, Y = by * SY - B;
+  const int za = std::max(0, z0 - B), zb = std::min(g.nz, std::min(g.nz, z0 + zlen) + B);
+  const int xa = std::max(0, X8), xb = std::min(g.nx, X8 + WB);
+  const int ya = std::max(0, Y), yb = std::min(g.ny, Y + c.rows);
+  for (int n = 0; n < h->nsrc; ++n) {
+    const fdtd::SourceDev& sd = h->src[n];
+    const bool in_z = sd.k >= za - 1 && sd.k <= zb;
+    if (in_z && (sd.kind != 0 || (sd.i >= xa && sd.i < xb && sd.j >= ya && sd.j < yb)))
+      return false;
+  }
+  if (!(xa < xb && ya < yb)) return false;
+  for (int kz = za / fdtd::kUniZ; kz <= (zb - 1) / fdtd::kUniZ; ++kz)
+    for (int ky = ya / fdtd::kUniY; ky <= (yb - 1) / fdtd::kUniY; ++ky)
+      for (int kx = xa / fdtd::kUniX; kx <= (xb - 1) / fdtd::kUniX; ++kx)
+        if (h->ublk_host[((size_t)kz * h->ub[1] + ky) * h->ub[0] + kx] == 0) return false;
+  return true;
+}
+
 const int* tile_order(fdtd_handle* h, const fdtd::TiledConfig& c) {
   if (!(c.width == 64 || c.pairs32) || h->ublk_host.empty() || !h->lean_enable) return nullptr;
   const long long key = ((((long long)h->version * 8 + c.blt) * 64 + c.rows) * 64 + c.z_chunks) *
                             2 + (c.pairs32 ? 1 : 0) + 4LL * c.width;
   if (key == h->order_key) return h->d_order;
   const Grid& g = h->g;
-  const int W = c.pairs32 ? 32 : c.width, B = c.blt;
-  const int SX = fdtd::tiled2_sx_w(W, B), SY = fdtd::tiled_sy(B, c.rows);
-  const int XB = fdtd::tiled2_xbase(B), WB = W + fdtd::kTiled2BoxPad;
   const int zlen = (g.nz + c.z_chunks - 1) / c.z_chunks;
   const dim3 gd = fdtd::tiled2_grid(c, g);
   const int ntile = (int)(gd.x * gd.y * gd.z);
   std::vector<int> mixed, lean;
   for (int q = 0; q < ntile; ++q) {
     const int bx = q % gd.x, by = (q / gd.x) % gd.y, bz = q / (gd.x * gd.y);
-    const int z0 = bz * zlen, X8 = (bx * SX + XB) & ~7, Y = by * SY - B;
-    const int za = std::max(0, z0 - B), zb = std::min(g.nz, std::min(g.nz, z0 + zlen) + B);
-    const int xa = std::max(0, X8), xb = std::min(g.nx, X8 + WB);
-    const int ya = std::max(0, Y), yb = std::min(g.ny, Y + c.rows);
-    bool ok = true;
-    for (int n = 0; n < h->nsrc && ok; ++n) {
-      const fdtd::SourceDev& sd = h->src[n];
-      const bool in_z = sd.k >= za - 1 && sd.k <= zb;
-      if (in_z && (sd.kind != 0 || (sd.i >= xa && sd.i < xb && sd.j >= ya && sd.j < yb))) ok = false;
-    }
-    if (ok && xa < xb && ya < yb)
-      for (int kz = za / fdtd::kUniZ; ok && kz <= (zb - 1) / fdtd::kUniZ; ++kz)
-        for (int ky = ya / fdtd::kUniY; ok && ky <= (yb - 1) / fdtd::kUniY; ++ky)
-          for (int kx = xa / fdtd::kUniX; ok && kx <= (xb - 1) / fdtd::kUniX; ++kx)
-            ok = h->ublk_host[((size_t)kz * h->ub[1] + ky) * h->ub[0] + kx] != 0;
-    (ok ? lean : mixed).push_back(q);
+    (tile_is_lean(h, c, bx, by, bz, zlen) ? lean : mixed).push_back(q);
   }
   h->order_key = key;
   if (mixed.empty() || lean.empty()) {
@@ -1715,17 +1725,22 @@ fdtd_status batch_items(fdtd_batch* b, const fdtd::TiledConfig& c, std::pair<int
     *out = it->second;
     return FDTD_OK;
   }
-  std::vector<std::pair<int, int4>> v;
+  // longest items first; at equal length the tiles that run the slower mixed march first
+  std::vector<std::pair<int, int4>> v;  // {2 * length + (lean-only ? 0 : 1), item}
   for (size_t i = 0; i < b->sims.size(); ++i) {
-    const Grid& g = b->sims[i]->g;
+    const fdtd_handle* h = b->sims[i];
+    const Grid& g = h->g;
     fdtd::TiledConfig ci = c;
     ci.z_chunks = sim_chunks(g, b->zlen);
     const dim3 gd = fdtd::tiled2_grid(ci, g);
-    const int len = (g.nz + ci.z_chunks - 1) / ci.z_chunks + 2 * c.blt;
+    const int zl = (g.nz + ci.z_chunks - 1) / ci.z_chunks;
+    const int len = zl + 2 * c.blt;
     for (unsigned bz = 0; bz < gd.z; ++bz)
       for (unsigned by = 0; by < gd.y; ++by)
-        for (unsigned bx = 0; bx < gd.x; ++bx)
-          v.push_back({len, make_int4((int)i, (int)bx, (int)by, (int)bz)});
+        for (unsigned bx = 0; bx < gd.x; ++bx) {
+          const bool lean = tile_is_lean(h, ci, (int)bx, (int)by, (int)bz, zl);
+          v.push_back({2 * len + (lean ? 0 : 1), make_int4((int)i, (int)bx, (int)by, (int)bz)});
+        }
   }
   std::stable_sort(v.begin(), v.end(),
                    [](const std::pair<int, int4>& a, const std::pair<int, int4>& b2) {
