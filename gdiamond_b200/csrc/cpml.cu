@@ -16,8 +16,8 @@
 // the non-PML solver; psi is stored only in the slabs of its axis (2L + 1 positions).
 //
 // One grid: cpml_e / cpml_h per step, monitors accumulated per step.  A batch of grids:
-// cpml_batch<E/H> cover every grid in one launch each (blockIdx.z = grid x block of planes,
-// arguments from a device array) and stage the monitor values for the deferred DFT.
+// cpml_e_batch / cpml_h_batch cover every grid in one launch each (blockIdx.z = grid * max_nz
+// + k, arguments from a device array) and stage the monitor values for the deferred DFT.
 #include "fdtd_kernels.cuh"
 
 namespace fdtd {
@@ -199,40 +199,27 @@ __device__ __forceinline__ void stage_cell(const CpmlSim& s, long long t, int i,
   }
 }
 
-// A batch: blockIdx.z = grid * zblocks + z block; each thread updates kBatchZ planes of its
-// (i, j) column.  The grid's arguments are copied into shared memory once per block, so the
-// per-cell code reads them from there rather than from the argument array.
-constexpr int kBatchZ = 8;
-
-__device__ __forceinline__ const CpmlSim& load_sim(const CpmlSim* sims, int g, CpmlSim* sh) {
-  static_assert(sizeof(CpmlSim) % 8 == 0, "8-byte words");
-  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(sims + g);
-  unsigned long long* dst = reinterpret_cast<unsigned long long*>(sh);
-  for (int q = threadIdx.y * 32 + threadIdx.x; q < (int)(sizeof(CpmlSim) / 8); q += 128)
-    dst[q] = src[q];
-  __syncthreads();
-  return *sh;
+// A batch: blockIdx.z = grid * max_nz + k over the grids' argument array.
+__global__ void __launch_bounds__(128) cpml_e_batch(const CpmlSim* sims, int max_nz,
+                                                    long long t_offset) {
+  const CpmlSim& s = sims[blockIdx.z / max_nz];
+  const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
+  const int k = (int)(blockIdx.z % max_nz);
+  if (i >= s.g.nx || j >= s.g.ny || k >= s.g.nz) return;
+  const long long t = s.t0 + t_offset;
+  if (interior(s.g, i, j, k)) e_cell(s.g, s.F, s.F, s.coef, s.mat, s.tab, s.S, t, s.dx, s.P, i, j, k);
+  if (s.M.n) stage_cell(s, t, i, j, k, true);
 }
 
-template <bool H>
-__global__ void __launch_bounds__(128) cpml_batch(const CpmlSim* sims, int zblocks,
-                                                  long long t_offset) {
-  __shared__ CpmlSim sh;
-  const CpmlSim& s = load_sim(sims, blockIdx.z / zblocks, &sh);
+__global__ void __launch_bounds__(128) cpml_h_batch(const CpmlSim* sims, int max_nz,
+                                                    long long t_offset) {
+  const CpmlSim& s = sims[blockIdx.z / max_nz];
   const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
-  if (i >= s.g.nx || j >= s.g.ny) return;
+  const int k = (int)(blockIdx.z % max_nz);
+  if (i >= s.g.nx || j >= s.g.ny || k >= s.g.nz) return;
   const long long t = s.t0 + t_offset;
-  const int k0 = (int)(blockIdx.z % zblocks) * kBatchZ;
-  const int k1 = min(s.g.nz, k0 + kBatchZ);
-  for (int k = k0; k < k1; ++k) {
-    if (interior(s.g, i, j, k)) {
-      if (H)
-        h_cell(s.g, s.F, s.F, s.coef, s.mat, s.tab, s.S, t, s.dx, s.P, i, j, k);
-      else
-        e_cell(s.g, s.F, s.F, s.coef, s.mat, s.tab, s.S, t, s.dx, s.P, i, j, k);
-    }
-    if (s.M.n) stage_cell(s, t, i, j, k, !H);
-  }
+  if (interior(s.g, i, j, k)) h_cell(s.g, s.F, s.F, s.coef, s.mat, s.tab, s.S, t, s.dx, s.P, i, j, k);
+  if (s.M.n) stage_cell(s, t, i, j, k, false);
 }
 
 // The shell companion: blockIdx.x indexes the block list; cells inside `inner` return.
@@ -284,18 +271,16 @@ cudaError_t launch_cpml_region(bool h_half, const Grid& g, const FieldPtrs& Fi,
 cudaError_t launch_cpml_batch_step(const CpmlSim* sims, int nsims, int max_nx, int max_ny,
                                    int max_nz, long long t_offset, cudaStream_t st) {
   if (nsims <= 0) return cudaSuccess;
-  if (max_nz <= 0) return cudaErrorInvalidValue;
-  const int zblocks = (max_nz + kBatchZ - 1) / kBatchZ;
-  if (zblocks > 65535) return cudaErrorInvalidValue;
+  if (max_nz <= 0 || max_nz > 65535) return cudaErrorInvalidValue;
   // grids per launch pair: blockIdx.z stays within its 65535 limit (grids are independent, so
   // each group's E launch before its H launch is all the order a step needs)
-  const int per = 65535 / zblocks;
+  const int per = 65535 / max_nz;
   const dim3 blk(32, 4);
   for (int g0 = 0; g0 < nsims; g0 += per) {
     const int n = nsims - g0 < per ? nsims - g0 : per;
-    const dim3 grd((max_nx + 31) / 32, (max_ny + 3) / 4, (unsigned)(n * zblocks));
-    cpml_batch<false><<<grd, blk, 0, st>>>(sims + g0, zblocks, t_offset);
-    cpml_batch<true><<<grd, blk, 0, st>>>(sims + g0, zblocks, t_offset);
+    const dim3 grd((max_nx + 31) / 32, (max_ny + 3) / 4, (unsigned)(n * max_nz));
+    cpml_e_batch<<<grd, blk, 0, st>>>(sims + g0, max_nz, t_offset);
+    cpml_h_batch<<<grd, blk, 0, st>>>(sims + g0, max_nz, t_offset);
   }
   return cudaGetLastError();
 }

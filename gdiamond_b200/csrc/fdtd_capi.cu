@@ -386,7 +386,8 @@ std::vector<fdtd::TiledConfig> candidates(const fdtd_handle* h) {
 // and monitors off, so the simulation state is not changed) and keeps the fastest per step.
 fdtd_status autotune(fdtd_handle* h, cudaStream_t st) {
   const auto key = std::make_tuple(h->g.nx, h->g.ny, h->g.nz,
-                                   h->storage * 1000000000LL + h->desc.min_blocks * 100000000LL +
+                                   (h->cpml_on ? 10000000000LL : 0LL) +
+                                       h->storage * 1000000000LL + h->desc.min_blocks * 100000000LL +
                                        h->desc.kernel * 1000000 + h->desc.blt * 10000 +
                                        h->desc.tile_rows * 100 + h->desc.z_chunks);
   {
@@ -399,6 +400,16 @@ fdtd_status autotune(fdtd_handle* h, cudaStream_t st) {
     }
   }
   std::vector<fdtd::TiledConfig> cands = candidates(h);
+  if (h->cpml_on) {
+    // With CPML layers the shell companion recomputes regions about 3 BLT cells deeper than
+    // the layers after every launch, so its cost grows with BLT while the timing below sees the
+    // tiled kernel alone: keep BLT <= 2 (by estimate the best total at 256^3 with 10-cell
+    // layers; BLT 6 measured slower overall).
+    std::vector<fdtd::TiledConfig> keep;
+    for (const auto& c : cands)
+      if (c.blt <= 2) keep.push_back(c);
+    if (!keep.empty()) cands.swap(keep);
+  }
   if (cands.empty()) return fail(h, FDTD_ERR_UNSUPPORTED, "no tiled configuration fits this grid");
   if (cands.size() == 1) {
     h->cfg = cands[0];
