@@ -2,7 +2,7 @@
 //
 // gDiamond has no learned component; this is the extension that maps a dielectric-box
 // parameterisation to a transmission spectrum, trained on spectra the batched FDTD solver
-// produces, with FDTD as both the fallback and the judge of its error.
+// produces, with FDTD as both the fallback and the ground truth for its error.
 //
 // Network per member: x -> [Linear -> GELU] x (L-1) -> Linear -> y, mean-squared-error loss.
 // FP32 master weights (updated by Adam) and BF16 copies (the GEMM operands); activations that

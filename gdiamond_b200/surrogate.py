@@ -22,7 +22,7 @@ sheet current is transverse (Jx): a z-directed current spread uniformly over a z
 curl and launches no wave along z.
 
 SpectrumSolver runs designs through the batched FDTD solver (the data generator, the fallback
-and the judge).  Surrogate wraps an ensemble of MLPs 6 -> 256 -> 256 -> 256 -> 64 (GELU, BF16
+and the ground truth).  Surrogate wraps an ensemble of MLPs 6 -> 256 -> 256 -> 256 -> 64 (GELU, BF16
 tensor-core GEMMs with FP32 accumulation, Adam) trained on the GPU by gdiamond_b200.MLP; a
 design whose ensemble disagreement (mean over the spectrum of the members' standard deviation,
 relative to the mean over the spectrum of |ensemble mean|) exceeds a threshold (1%) is sent to

@@ -2,7 +2,7 @@
 
 The bar is bit-exactness: every multiply and add in the kernels is separately rounded, as in
 the reference's CPU build, so fields and FP64 monitor sums must equal the oracle's bit for bit.
-The north-star tolerance (relative L2 <= 1e-5 per component) is asserted as well, so a
+The FP32 tolerance of the workload (relative L2 <= 1e-5 per component) is asserted as well, so a
 failure reports both.  Cases:
   * the reference unit test (unittests/checker_gpu.cu): 100^3, 100 steps, the reference
     constructor's coefficients and its Mz source -> the golden SHA-256 of update_FDTD_seq;
@@ -29,7 +29,7 @@ from gdiamond_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REL_L2_TOL = 1e-5  # north-star FP32 tolerance (relative L2 per component)
+REL_L2_TOL = 1e-5  # FP32 tolerance (relative L2 per component)
 
 
 def sha(a):

@@ -1,6 +1,6 @@
 """The spectrum surrogate end to end on a small grid (32^3, T=300, 16 frequencies).
 
-* the batched FDTD spectrum solver (data generator, fallback, judge) against the oracle: the
+* the batched FDTD spectrum solver (data generator, fallback, ground truth) against the oracle: the
   plane-summed Ex DFT and the Poynting flux (the flux monitor's definition, oracle.flux) of a
   design run in a batch equal the oracle's for the same permittivity, and a box of eps 1
   transmits exactly 1;
