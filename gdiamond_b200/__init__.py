@@ -43,7 +43,8 @@ EXPORTS = (
     "fdtd_storage_bytes", "fdtd_set_step", "fdtd_set_dft", "fdtd_component_bytes",
     "fdtd_dft_folds", "fdtd_set_fast_path", "fdtd_fast_path", "fdtd_add_flux_monitor",
     "fdtd_get_flux", "fdtd_get_flux_device", "fdtd_flux_monitor_ids", "fdtd_debug_fail_copy",
-    "fdtd_set_cpml", "fdtd_get_cpml_profile",
+    "fdtd_set_cpml", "fdtd_get_cpml_profile", "fdtd_cpml_psi_bytes", "fdtd_get_cpml_psi",
+    "fdtd_set_cpml_psi",
 )
 
 
@@ -113,6 +114,9 @@ def library():
             "fdtd_dft_folds": ([V, P(C.c_int32)], C.c_int),
             "fdtd_set_fast_path": ([V, C.c_int32], C.c_int),
             "fdtd_set_cpml": ([V, P(_Cpml)], C.c_int),
+            "fdtd_cpml_psi_bytes": ([V, C.c_int32, P(C.c_int64)], C.c_int),
+            "fdtd_get_cpml_psi": ([V, C.c_int32, V], C.c_int),
+            "fdtd_set_cpml_psi": ([V, C.c_int32, V], C.c_int),
             "fdtd_get_cpml_profile": ([V, C.c_int32, C.c_int32, P(C.c_float), P(C.c_float),
                                        P(C.c_float), P(C.c_int32)], C.c_int),
             "fdtd_debug_fail_copy": ([V, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64],
@@ -362,6 +366,27 @@ class Simulation:
                   float(alpha_max), float(np.float32(dt)))
         self._check(self._L.fdtd_set_cpml(self._h, C.byref(d)))
 
+    def cpml_state(self):
+        """The twelve CPML psi arrays (float32, flat; None without layers)."""
+        out = []
+        for q in range(12):
+            n = C.c_int64()
+            if self._L.fdtd_cpml_psi_bytes(self._h, q, C.byref(n)) != 0:
+                return None
+            a = np.empty(n.value // 4, np.float32)
+            self._check(self._L.fdtd_get_cpml_psi(self._h, q, a.ctypes.data_as(C.c_void_p)))
+            out.append(a)
+        return out
+
+    def set_cpml_state(self, psi):
+        for q, a in enumerate(psi):
+            a = np.ascontiguousarray(a, np.float32)
+            n = C.c_int64()
+            self._check(self._L.fdtd_cpml_psi_bytes(self._h, q, C.byref(n)))
+            if a.nbytes != n.value:
+                raise ValueError("CPML state of other layers")
+            self._check(self._L.fdtd_set_cpml_psi(self._h, q, a.ctypes.data_as(C.c_void_p)))
+
     def cpml_tables(self):
         """[axis][kind] = (slot, b, a, inv_kappa) of the layers (kind 0: E positions, 1: H)."""
         out = []
@@ -475,7 +500,7 @@ class Simulation:
 
     def checkpoint(self):
         """The whole state as host arrays: step counter, the current field set in its storage
-        format (raw), every monitor's sums.  restore() on a handle with the same shape,
+        format (raw), every monitor's sums, the CPML psi arrays when layers are on.  restore() on a handle with the same shape,
         storage, sources and monitors continues bit for bit."""
         import torch
         self.sync()
@@ -490,7 +515,8 @@ class Simulation:
             self.sync()
             fields.append(buf.cpu().numpy().copy())
         return {"t": self.t, "shape": self.shape, "esz": esz, "fields": fields,
-                "dft": [self.get_dft(m) for m in range(self.n_monitors)]}
+                "dft": [self.get_dft(m) for m in range(self.n_monitors)],
+                "cpml_psi": self.cpml_state()}
 
     def restore(self, ckpt):
         import torch
@@ -499,6 +525,9 @@ class Simulation:
             raise ValueError("checkpoint of another shape or storage")
         if len(ckpt["dft"]) != self.n_monitors:
             raise ValueError("checkpoint with another set of monitors")
+        psi = ckpt.get("cpml_psi")
+        if (psi is None) != (self.cpml_state() is None):
+            raise ValueError("checkpoint and handle differ in CPML layers")
         nz = self.shape[2]
         self.sync()
         for c, f in enumerate(ckpt["fields"]):
@@ -507,6 +536,8 @@ class Simulation:
             self.sync()
         for m, (re, im) in enumerate(ckpt["dft"]):
             self.set_dft(m, re, im)
+        if psi is not None:
+            self.set_cpml_state(psi)
         self._check(self._L.fdtd_set_step(self._h, int(ckpt["t"])))
 
     def get_dft_device(self, monitor_id, re_ptr, im_ptr, stream=None):

@@ -844,7 +844,11 @@ fdtd_status cpml_region_blocks(fdtd_handle* h, int r, std::pair<int4*, int>* out
   }
   int4* d = nullptr;
   CUDA_TRY(h, cudaMalloc(&d, std::max<size_t>(v.size(), 1) * sizeof(int4)));
-  CUDA_TRY(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  const cudaError_t e = cudaMemcpy(d, v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    return fail(h, FDTD_ERR_CUDA, "CPML block list upload failed: %s", cudaGetErrorString(e));
+  }
   h->cpml_blocks[r] = {d, (int)v.size()};
   *out = h->cpml_blocks[r];
   return FDTD_OK;
@@ -854,9 +858,16 @@ fdtd_status cpml_region_blocks(fdtd_handle* h, int r, std::pair<int4*, int>* out
 fdtd_status cpml_companion(fdtd_handle* h, int k, int src, int dst, long long t,
                            const fdtd::Sources& S, const fdtd::Monitors& M, cudaStream_t st,
                            int* launches) {
-  if (k > 1 && !h->cpml_scratch[0]) {
+  if (k > 1 && !h->cpml_scratch[0]) {  // all six or none
     for (int c = 0; c < 6; ++c)
-      CUDA_TRY(h, cudaMalloc(&h->cpml_scratch[c], h->cells * sizeof(float)));
+      if (cudaMalloc(&h->cpml_scratch[c], h->cells * sizeof(float)) != cudaSuccess) {
+        for (int q = 0; q < 6; ++q) {
+          cudaFree(h->cpml_scratch[q]);
+          h->cpml_scratch[q] = nullptr;
+        }
+        cudaGetLastError();
+        return fail(h, FDTD_ERR_OOM, "CPML companion field set allocation failed");
+      }
   }
   fdtd::FieldPtrs A, B, C;
   for (int c = 0; c < 6; ++c) {
@@ -1628,6 +1639,28 @@ fdtd_status fdtd_get_cpml_profile(const fdtd_handle* h, int32_t axis, int32_t h_
   if (inv_kappa) std::copy(pr[2].begin(), pr[2].end(), inv_kappa);
   if (slot) std::copy(h->cpml_slot[axis][k].begin(), h->cpml_slot[axis][k].end(), slot);
   (void)n;
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_cpml_psi_bytes(const fdtd_handle* h, int32_t q, int64_t* bytes) {
+  if (!h || !bytes || q < 0 || q > 11 || !h->cpml_on) return FDTD_ERR_INVALID_ARG;
+  *bytes = (int64_t)cpml_psi_bytes(h, q);
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_get_cpml_psi(fdtd_handle* h, int32_t q, void* host_out) {
+  if (!h || !host_out || q < 0 || q > 11 || !h->cpml_on) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  CUDA_TRY(h, cudaMemcpy(host_out, h->cpml_psi[q], cpml_psi_bytes(h, q), cudaMemcpyDeviceToHost));
+  return FDTD_OK;
+}
+
+fdtd_status fdtd_set_cpml_psi(fdtd_handle* h, int32_t q, const void* host_in) {
+  if (!h || !host_in || q < 0 || q > 11 || !h->cpml_on) return FDTD_ERR_INVALID_ARG;
+  DeviceGuard dg(h->desc.device);
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  CUDA_TRY(h, cudaMemcpy(h->cpml_psi[q], host_in, cpml_psi_bytes(h, q), cudaMemcpyHostToDevice));
   return FDTD_OK;
 }
 

@@ -197,6 +197,13 @@ typedef struct fdtd_cpml_desc {
   float dt;            /* time step of the run (the reference's 0.05) */
 } fdtd_cpml_desc;
 fdtd_status fdtd_set_cpml(fdtd_handle* h, const fdtd_cpml_desc* desc);
+/* The layers' auxiliary state, for checkpoint / resume (no reference counterpart): psi array q,
+ * 0..5 of the E updates (exy exz eyz eyx ezx ezy), 6..11 of the H updates (hxz hxy hyx hyz hzy
+ * hzx), FP32 in the slabs of its axis; *bytes = its size.  Synchronous; INVALID_ARG without
+ * layers. */
+fdtd_status fdtd_cpml_psi_bytes(const fdtd_handle* h, int32_t q, int64_t* bytes);
+fdtd_status fdtd_get_cpml_psi(fdtd_handle* h, int32_t q, void* host_out);
+fdtd_status fdtd_set_cpml_psi(fdtd_handle* h, int32_t q, const void* host_in);
 /* The tabulated profile of one axis (0 x, 1 y, 2 z) at E positions (h_positions = 0) or H
  * positions (1): b, a, 1/kappa and the psi slot (-1 outside the layer), Nx/Ny/Nz entries each
  * (any pointer may be NULL). */
