@@ -12,8 +12,10 @@ Metric: Gcell-updates/s (Nx*Ny*Nz*T / s, boundary cells included, as the referen
 gDiamond/gdiamond.hpp:1253).  `value` times the device-resident run (CUDA events on the
 launching stream, max over ranks); `e2e` times the same run through the C-ABI with host
 buffers: coefficient upload (12 FP32 arrays from pinned memory), reset, 1000 steps, download
-of the 6 fields and the monitor sums.  Under torchrun each rank runs its own replica (the grid
-is one object; no data-path collective): `scaling` is weak.
+of the 6 fields and the monitor sums.  Under torchrun (N ranks) the grid grows to
+256 x 256 x 256N and is split into z-slabs, one per rank, with one halo exchange per tiled
+launch (--parallelism zslab, the default), or each rank runs its own 256^3 replica
+(--parallelism replicas): `scaling` is weak either way.
 
 --impl reference times the reference's own CPU path, gDiamond::update_FDTD_omp, compiled from
 the reference sources (oracle/_ref/libgdref.so) on this host's cores, on a bounded number of
@@ -454,7 +456,8 @@ def run_ours(args):
         for name, fn in (("mixed", lambda: mixed_results(args)),
                          ("batched", lambda: batched_results(args, ("f16e", "f32"),
                                                              one_at_a_time=False)),
-                         ("reference_gpu", reference_gpu_results)):
+                         ("reference_gpu", reference_gpu_results),
+                         ("cpml", cpml_results)):
             try:
                 t0 = time.perf_counter()
                 extra[name] = fn()
@@ -698,6 +701,50 @@ def fp16_scales(probe, ncell, T, every=2, headroom=2048.0, k_src=None, halfwidth
 def run_mixed(args):
     print(json.dumps(mixed_results(args)))
     return 0
+
+
+def cpml_results(L=10, reps=2):
+    """The 256^3 workload (Gaussian Jz at the centre, 8-frequency Ez DFT, 1000 steps) with CPML
+    layers of L cells on every face: Gcell-updates/s of the tiled kernel with the shell
+    companion and of the per-step CPML kernels (the naive kernel choice), CUDA events on the
+    stepping stream, and whether their final fields and DFT sums agree bit for bit."""
+    import torch
+    import gdiamond_b200 as gd
+    from gdiamond_b200 import workloads as W
+    nx, ny, nz = SHAPE
+    T = T_STEPS
+    wave = W.gaussian_wave(T)
+    freqs = W.source_band(N_FREQS)
+    out, finals = {}, {}
+    for name, kernel in (("companion", "auto"), ("per_step", "naive")):
+        sim = gd.Simulation(nx, ny, nz, kernel=kernel)
+        sim.set_coefficients(W.vacuum_coefficients(SHAPE))
+        sim.set_cpml(thickness=L)
+        sim.set_sources([dict(component="Jz", wave=wave, i=nx // 2, j=ny // 2, k=nz // 2)])
+        mid = sim.add_dft_monitor("Ez", nz // 2, freqs, scale=1.0)
+        stream = torch.cuda.Stream()
+        sim.step(T, stream=stream)  # tunes (the companion's tiled kernel) outside the timing
+        stream.synchronize()
+        ms = []
+        for _ in range(reps):
+            sim.reset()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.step(T, stream=stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        sim.sync()
+        cfg = sim.config()
+        finals[name] = ([sim.get_field(c) for c in range(6)], sim.get_dft(mid))
+        out[name] = {"gcells": nx * ny * nz * T / (min(ms) / 1e3) / 1e9, "ms": ms,
+                     "kernel": cfg["kernel"], "blt": cfg["blt"], "tile_rows": cfg["tile_rows"]}
+        sim.close()
+    (fa, da), (fb, db) = finals["companion"], finals["per_step"]
+    same = all(np.array_equal(a.view(np.uint32), b.view(np.uint32)) for a, b in zip(fa, fb))
+    same = same and all(np.array_equal(a, b) for a, b in zip(da, db))
+    return {"metric": "Gcell-updates/s with CPML layers", "workload": f"{WORKLOAD}_cpml{L}",
+            "results": out, "companion_equals_per_step_bitwise": bool(same)}
 
 
 def mixed_results(args, storages=("f32", "bf16", "f16", "f16e")):
