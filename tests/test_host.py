@@ -98,6 +98,9 @@ def test_null_handle_calls_return_invalid_arg():
     assert L.fdtd_step(None, 1, None) == 1
     assert L.fdtd_sync(None) == 1
     assert L.fdtd_destroy(None) == 1
+    assert L.fdtd_cpml_psi_bytes(None, 0, None) == 1
+    assert L.fdtd_get_cpml_psi(None, 0, None) == 1
+    assert L.fdtd_set_cpml_psi(None, 0, None) == 1
 
 
 def test_surrogate_fallback_bucket_sizes():
@@ -106,3 +109,18 @@ def test_surrogate_fallback_bucket_sizes():
     assert [S.bucket(n, 256) for n in (1, 3, 4, 5, 9, 100, 256, 300)] == \
         [4, 4, 4, 8, 16, 128, 256, 256]
     assert S.bucket(7, 6) == 6
+
+
+def test_surrogate_solver_boundary_arguments():
+    """CPML layers must leave the source and flux planes outside them (checked before any
+    device work); 8-cell layers are the default with CPML and keep the stated z = 10 / z = 86
+    planes of the 96^3 grid outside."""
+    import pytest
+    from gdiamond_b200 import surrogate as S
+    with pytest.raises(ValueError):
+        S.SpectrumSolver(boundary="cpml", t_pml=10)  # z = 86 lies in a 10-cell top layer
+    with pytest.raises(ValueError):
+        S.SpectrumSolver(boundary="cpml", source_k=6)  # z = 6 lies in the bottom layer
+    with pytest.raises(ValueError):
+        S.SpectrumSolver(boundary="absorbing")
+    assert 8 <= S.SOURCE_K and S.MONITOR_K <= S.SHAPE[2] - 2 - 8
