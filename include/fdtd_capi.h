@@ -322,9 +322,11 @@ fdtd_status fdtd_build_material_map_noalloc(const float* const* coef12_dev, int6
 /* ---------------------------------------------------------------- batches
  * Many independent simulations advanced together.  The reference runs one grid per call;
  * here a batch groups existing handles (same device and storage, coefficients compressed to a
- * material map) and fdtd_batch_step advances all of them with one persistent launch of the
- * tiled x-pair kernel per BLT steps: CTAs pull (simulation, tile) work items, longest first,
- * from an atomic queue, so grids of uneven size share the GPU without per-grid launches. */
+ * material map, CPML layers on all of them or on none) and fdtd_batch_step advances all of them
+ * with one persistent launch of the tiled x-pair kernel per BLT steps: CTAs pull (simulation,
+ * tile) work items, longest first, from an atomic queue, so grids of uneven size share the GPU
+ * without per-grid launches.  A batch with CPML layers instead runs one E and one H launch per
+ * step over every grid. */
 typedef struct fdtd_batch fdtd_batch;
 
 fdtd_status fdtd_batch_create(fdtd_handle* const* sims, int32_t n, fdtd_batch** out);
